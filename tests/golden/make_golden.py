@@ -1,0 +1,304 @@
+"""Generates the golden fixtures under tests/golden/ by RUNNING THE REFERENCE.
+
+The reference (saurabh-jain/registration, py-lddmm/) is Python 2 code over an
+f2py Fortran module.  In this container there is neither a Python 2
+interpreter nor a Fortran compiler, so this script:
+
+1. loads the reference's own Python modules from the read-only checkout
+   (default /root/reference/py-lddmm, or $LDDMM_REFERENCE_DIR) after three
+   mechanical, semantics-preserving source rewrites done in memory
+   (nothing is copied into this repository):
+     - tabs expanded to 8-column stops (Python 2 indentation rule);
+     - ``print x, y`` statements turned into ``print(x, y)`` calls;
+     - ``== None`` / ``!= None`` turned into ``is None`` / ``is not None``
+       (what the comparison returned for arrays under the numpy of the
+       Python 2 era; modern numpy compares element-wise instead);
+2. registers the oracle (``oracle.FortShim``, a C/OpenMP restatement of
+   kernelFunctions.f90) as the module ``kernelFunctions_fort`` that the
+   reference imports, and a stub ``gaussianDiffeons`` (imported by
+   pointEvolution.py but unused by the landmark functions);
+3. runs the reference's Kernel / pointEvolution / surfaces / curves /
+   surfaceMatching / curveMatching / conjugateGradient code on small seeded
+   inputs, and additionally evaluates the reference's own dense numpy kernel
+   matrices (kernelMatrixGauss / kernelMatrixLaplacian) as an independent
+   check of the restated Fortran loops.
+
+VTK writers are replaced by no-ops (output only; they do not change the
+optimisation state).  Run from the repository root:
+
+    python tests/golden/make_golden.py
+"""
+import io
+import os
+import re
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from registration_b200 import geometry as geo  # noqa: E402
+
+REF = os.environ.get("LDDMM_REFERENCE_DIR", "/root/reference/py-lddmm")
+
+_PRINT = re.compile(r"^(\s*)print(\s+(.*))?$")
+
+
+def _py3_source(text):
+    out = []
+    for line in text.expandtabs(8).splitlines():
+        m = _PRINT.match(line)
+        if m and not line.strip().startswith("print("):
+            body = (m.group(3) or "").rstrip()
+            line = "%sprint(%s)" % (m.group(1), body.rstrip(","))
+        line = re.sub(r"!=\s*None\b", " is not None", line)
+        line = re.sub(r"==\s*None\b", " is None", line)
+        out.append(line)
+    return "\n".join(out) + "\n"
+
+
+def load_reference(names=("kernelFunctions", "affineBasis", "pointEvolution", "surfaces", "curves",
+                           "matchingParam", "grid", "conjugateGradient", "gradientDescent", "surfaceMatching",
+                           "curveMatching")):
+    sys.modules["kernelFunctions_fort"] = oracle.FortShim()
+    sys.modules["gaussianDiffeons"] = types.ModuleType("gaussianDiffeons")
+    mods = {}
+    for nm in names:
+        path = os.path.join(REF, nm + ".py")
+        with open(path) as fh:
+            src = _py3_source(fh.read())
+        mod = types.ModuleType(nm)
+        mod.__file__ = path
+        sys.modules[nm] = mod
+        exec(compile(src, path, "exec"), mod.__dict__)
+        mods[nm] = mod
+    # output-only writers -> no-ops
+    mods["surfaces"].Surface.saveVTK = lambda self, *a, **k: None
+    mods["surfaces"].Surface.saveVTK2 = lambda self, *a, **k: None
+    mods["curves"].Curve.saveVTK = lambda self, *a, **k: None
+    mods["grid"].Grid.saveVTK = lambda self, *a, **k: None
+    return mods
+
+
+def dense_applyk(R, kname, sigma, order, x, y, beta):
+    """Reference dense path: kernelMatrix* (kernelFunctions.py:10-198) times beta."""
+    kf = R["kernelFunctions"]
+    if kname == "gauss":
+        K, _ = kf.kernelMatrixGauss(y, firstVar=x, par=[sigma])
+    else:
+        K, _ = kf.kernelMatrixLaplacian(y, firstVar=x, par=[sigma, order])
+    return K @ beta
+
+
+def dense_applydifft(R, kname, sigma, order, x, y, a1, a2):
+    """Reference dense K' matrix (diff=True) with the formula kept beside the
+    f2py call at kernelFunctions.py:424-430."""
+    kf = R["kernelFunctions"]
+    if kname == "gauss":
+        r, _ = kf.kernelMatrixGauss(y, firstVar=x, par=[sigma], diff=True)
+    else:
+        r, _ = kf.kernelMatrixLaplacian(y, firstVar=x, par=[sigma, order], diff=True)
+    a = sum(a1[i] @ a2[i].T for i in range(a1.shape[0]))
+    g1 = r * a
+    return 2 * (x * g1.sum(axis=1)[:, None] - g1 @ y)
+
+
+def kernel_cases(R, out):
+    kf = R["kernelFunctions"]
+    rng = np.random.default_rng(1234)
+    cases = []
+    for kname, order in [("gauss", 10), ("laplacian", 0), ("laplacian", 1), ("laplacian", 2), ("laplacian", 3),
+                         ("laplacian", 4)]:
+        for d in (2, 3):
+            for dimb in (1, 3):
+                n, m = 37, 53
+                sigma = 0.35
+                x = rng.uniform(0, 1, (n, d))
+                y = rng.uniform(0, 1, (m, d))
+                y[:5] = x[:5]          # exact coincidences: zero-distance branch
+                y[5] = x[6] + 1e-10    # below the 1e-8 threshold
+                beta = rng.standard_normal((m, dimb))
+                K = kf.Kernel(name=kname, sigma=sigma, order=order)
+                fk = K.applyK(y, beta, firstVar=x)
+                fself = K.applyK(x, rng.standard_normal((n, dimb)))
+                tag = "%s%d_d%d_b%d" % (kname, K.order, d, dimb)
+                out["applyk_x_" + tag] = x
+                out["applyk_y_" + tag] = y
+                out["applyk_beta_" + tag] = beta
+                out["applyk_f_" + tag] = fk
+                oracle.set_exact_coeffs(True)
+                out["applyk_dense_" + tag] = dense_applyk(R, kname, sigma, K.order, x, y, beta)
+                out["applyk_exact_" + tag] = oracle.applyk(x, y, beta, sigma, K.order)
+                oracle.set_exact_coeffs(False)
+                if K.order > 0:
+                    for na in (1, 3):
+                        a1 = rng.standard_normal((na, n, dimb))
+                        a2 = rng.standard_normal((na, m, dimb))
+                        fd = K.applyDiffKT(y, a1, a2, firstVar=x)
+                        t2 = tag + "_na%d" % na
+                        out["difft_a1_" + t2] = a1
+                        out["difft_a2_" + t2] = a2
+                        out["difft_f_" + t2] = fd
+                        oracle.set_exact_coeffs(True)
+                        out["difft_dense_" + t2] = dense_applydifft(R, kname, sigma, K.order, x, y, a1, a2)
+                        out["difft_exact_" + t2] = oracle.applykdifft(x, y, a1, a2, sigma, K.order)
+                        oracle.set_exact_coeffs(False)
+                cases.append(tag)
+                del fself
+    out["kernel_cases"] = np.array(cases)
+
+
+def evolution_cases(R, out):
+    kf = R["kernelFunctions"]
+    ev = R["pointEvolution"]
+    rng = np.random.default_rng(99)
+    for kname, sigma in [("gauss", 0.5), ("laplacian", 0.6)]:
+        N, d, T = 40, 3, 5
+        x0 = rng.uniform(-1, 1, (N, d))
+        at = 0.3 * rng.standard_normal((T, N, d))
+        px1 = rng.standard_normal((N, d))
+        K = kf.Kernel(name=kname, sigma=sigma)
+        xt = ev.landmarkDirectEvolutionEuler(x0, at, K)
+        grid = rng.uniform(-1, 1, (17, d))
+        xt2, yt, Jt = ev.landmarkDirectEvolutionEuler(x0, at, K, withJacobian=True, withPointSet=grid)
+        n0 = rng.standard_normal((N, d))
+        xt3, nt = ev.landmarkDirectEvolutionEuler(x0, at, K, withNormals=n0)
+        xt4, Jt4 = ev.landmarkDirectEvolutionEuler(x0, at, K, withJacobian=True)
+        pxt, xt5 = ev.landmarkHamiltonianCovector(x0, at, px1, K, 0.7)
+        dat, xt6, pxt6 = ev.landmarkHamiltonianGradient(x0, at, px1, K, 0.7, getCovector=True)
+        xte, ate = ev.landmarkEPDiff(T, x0, at[0], K)
+        p = "evo_%s_" % kname
+        for k, v in dict(x0=x0, at=at, px1=px1, xt=xt, grid=grid, yt=yt, Jt=Jt, n0=n0, nt=nt, Jt_self=Jt4,
+                         pxt=pxt, dat=dat, xt_epdiff=xte, at_epdiff=ate).items():
+            out[p + k] = v
+        out[p + "sigma"] = sigma
+
+
+def surface_cases(R, out):
+    kf = R["kernelFunctions"]
+    sf = R["surfaces"]
+    rng = np.random.default_rng(7)
+    v, f = geo.icosphere(1)
+    vt = geo.bumped_sphere(v, f, 4, 0.5, 0.2, rng)
+    vd = v + 0.05 * rng.standard_normal(v.shape)
+    fv1 = sf.Surface(FV=[f, vt])
+    fvD = sf.Surface(FV=[f, vd])
+    out["surf_faces"] = f
+    out["surf_vdef"] = vd
+    out["surf_vtgt"] = vt
+    out["surf_centers"] = fvD.centers
+    out["surf_surfel"] = fvD.surfel
+    for kname, sig in [("gauss", 0.4), ("laplacian", 0.5)]:
+        K = kf.Kernel(name=kname, sigma=sig)
+        for err in ("current", "measure", "varifold"):
+            p = "surf_%s_%s_" % (err, kname)
+            out[p + "norm0"] = getattr(sf, err + "Norm0")(fv1, K)
+            out[p + "normdef"] = getattr(sf, err + "NormDef")(fvD, fv1, K)
+            out[p + "grad"] = getattr(sf, err + "NormGradient")(fvD, fv1, K)
+
+
+def curve_cases(R, out):
+    kf = R["kernelFunctions"]
+    cv = R["curves"]
+    rng = np.random.default_rng(11)
+    v, f = geo.ellipse_curve(48)
+    vt, _ = geo.bumped_curve(v, 4, 0.3, 0.1, rng)
+    vd = v + 0.03 * rng.standard_normal(v.shape)
+    fv1 = cv.Curve(pointSet=vt)
+    fvD = cv.Curve(pointSet=vd)
+    out["curve_vdef"] = vd
+    out["curve_vtgt"] = vt
+    for kname, sig in [("gauss", 0.5), ("laplacian", 0.5)]:
+        K = kf.Kernel(name=kname, sigma=sig)
+        for err in ("current", "measure"):
+            p = "curve_%s_%s_" % (err, kname)
+            out[p + "norm0"] = getattr(cv, err + "Norm0")(fv1, K)
+            out[p + "normdef"] = getattr(cv, err + "NormDef")(fvD, fv1, K)
+            out[p + "grad"] = getattr(cv, err + "NormGradient")(fvD, fv1, K)
+
+
+def _record_trace(obj):
+    trace = []
+    orig = obj.acceptVarTry
+
+    def accept():
+        orig()
+        trace.append(float(obj.obj))
+
+    obj.acceptVarTry = accept
+    return trace
+
+
+def matching_cases(R, out):
+    kf = R["kernelFunctions"]
+    sf = R["surfaces"]
+    cv = R["curves"]
+    SM = R["surfaceMatching"]
+    CM = R["curveMatching"]
+    tmp = tempfile.mkdtemp(prefix="lddmm_golden_")
+    # surface matching, icosphere subdivision 2 (162 vertices)
+    rng = np.random.default_rng(5)
+    v, f = geo.icosphere(2)
+    vt = geo.bumped_sphere(v, f, 6, 0.35, 0.15, rng)
+    out["sm_faces"] = f
+    out["sm_v0"] = v
+    out["sm_v1"] = vt
+    for err, sdist in [("varifold", 0.3), ("current", 0.3), ("measure", 0.3)]:
+        param = SM.SurfaceMatchingParam(timeStep=0.2, KparDiff=kf.Kernel(name="gauss", sigma=0.4),
+                                        KparDist=kf.Kernel(name="gauss", sigma=sdist), sigmaError=0.5,
+                                        errorType=err)
+        sm = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v]), Target=sf.Surface(FV=[f, vt]), param=param,
+                                maxIter=6, testGradient=False, outputDir=tmp)
+        sm.saveRate = 10 ** 9   # skip the output-only branch of endOfIteration
+        trace = _record_trace(sm)
+        sm.optimizeMatching()
+        p = "sm_%s_" % err
+        out[p + "trace"] = np.array([float(sm.obj0)] + trace)
+        out[p + "at"] = sm.at
+        out[p + "gradEps"] = sm.gradEps
+    # curve matching, 64-vertex ellipse (curveMatching.py: cg with epsInit=10)
+    rng = np.random.default_rng(3)
+    v, f = geo.ellipse_curve(64)
+    vt, _ = geo.bumped_curve(v, 4, 0.3, 0.1, rng)
+    out["cm_v0"] = v
+    out["cm_v1"] = vt
+    for err in ("current", "measure"):
+        param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5),
+                                      KparDist=kf.Kernel(name="gauss", sigma=0.5), sigmaError=1.0, errorType=err)
+        stdout = sys.stdout
+        sys.stdout = io.StringIO()   # the reference prints on every objectiveFun
+        try:
+            cm = CM.CurveMatching(Template=cv.Curve(pointSet=v), Target=cv.Curve(pointSet=vt), param=param,
+                                  maxIter=8, saveRate=0, outputDir=tmp)
+            trace = _record_trace(cm)
+            cm.optimizeMatching()
+        finally:
+            sys.stdout = stdout
+        p = "cm_%s_" % err
+        out[p + "trace"] = np.array([float(cm.obj0)] + trace)
+        out[p + "at"] = cm.at
+        out[p + "gradEps"] = cm.gradEps
+
+
+def main():
+    oracle.build()
+    oracle.set_num_threads(4)
+    R = load_reference()
+    out = {}
+    kernel_cases(R, out)
+    evolution_cases(R, out)
+    surface_cases(R, out)
+    curve_cases(R, out)
+    matching_cases(R, out)
+    dst = os.path.join(HERE, "reference_golden.npz")
+    np.savez_compressed(dst, **out)
+    print("wrote %s (%d arrays, %.1f KB)" % (dst, len(out), os.path.getsize(dst) / 1024.0))
+
+
+if __name__ == "__main__":
+    main()
