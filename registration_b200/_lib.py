@@ -1,0 +1,71 @@
+"""ctypes binding of liblddmm_b200.so (the C ABI declared in include/lddmm_b200.h).
+
+The shared library is built in-tree by ``python -m registration_b200.build``.
+There is no CPU fallback: if the library or a CUDA device is missing, every
+operation raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblddmm_b200.so")
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I = ctypes.c_int
+_D = ctypes.c_double
+_SZ = ctypes.c_size_t
+
+# name -> (restype, argtypes); mirrors include/lddmm_b200.h
+SIGNATURES = {
+    "lddmm_last_error": (ctypes.c_char_p, []),
+    "lddmm_abi_version": (_I, []),
+    "lddmm_applyk_f32c_workspace": (_SZ, [_I64, _I64, _I, _I]),
+    "lddmm_applyk_f64_workspace": (_SZ, [_I64, _I64, _I, _I]),
+    "lddmm_applyk_f32c": (_I, [_P, _I64, _P, _I64, _P, _I, _I, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applyk_f64": (_I, [_P, _I64, _P, _I64, _P, _I, _I, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdifft_f32c_workspace": (_SZ, [_I64, _I64, _I, _I, _I]),
+    "lddmm_applykdifft_f64_workspace": (_SZ, [_I64, _I64, _I, _I, _I]),
+    "lddmm_applykdifft_f32c": (_I, [_P, _I64, _P, _I64, _P, _P, _I, _I, _I, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdifft_f64": (_I, [_P, _I64, _P, _I64, _P, _P, _I, _I, _I, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_probe_launch": (_I, [_I, _I, _I, _I, _P, _P]),
+}
+
+ERRORS = {-1: "invalid argument", -2: "workspace too small", -3: "CUDA error", -4: "unsupported"}
+
+_lib = None
+
+
+class LddmmError(RuntimeError):
+    pass
+
+
+def load():
+    """Loads the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LddmmError("liblddmm_b200.so not found at %s; build it with "
+                             "`python -m registration_b200.build` (no CPU fallback exists)" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def call(name, *args):
+    rc = getattr(load(), name)(*args)
+    if rc != 0:
+        msg = load().lddmm_last_error().decode(errors="replace")
+        kind = ERRORS.get(rc, "error %d" % rc)
+        if rc == -1:
+            raise ValueError("%s: %s (%s)" % (name, msg, kind))
+        raise LddmmError("%s: %s (%s)" % (name, msg, kind))
+    return rc
+
+
+def query(name, *args):
+    return int(getattr(load(), name)(*args))

@@ -1,0 +1,54 @@
+// Diagnostic kernels that measure this GPU's FP32 FMA and MUFU ex2 issue rates.
+// bench.py times them to get the measured peaks that the kernel-sum roofline
+// fractions are quoted against.
+#include "host.h"
+
+namespace lddmm {
+
+// 8 independent FMA chains per thread, unrolled: 8*iters FFMA per thread.
+static __global__ void probe_ffma_kernel(float* out, int iters, float a, float b) {
+    float x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = (threadIdx.x + j) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = fmaf(x[j], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += x[j];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// 8 independent ex2 chains per thread: 8*iters MUFU.EX2 per thread.
+static __global__ void probe_ex2_kernel(float* out, int iters) {
+    float x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = (threadIdx.x + j) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = ex2(-x[j]);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += x[j];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace lddmm
+
+extern "C" LDDMM_API int lddmm_probe_launch(int what, int blocks, int threads, int iters, float* out,
+                                            lddmm_stream_t stream) {
+    using namespace lddmm;
+    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || (what != 0 && what != 1)) {
+        set_error("probe: invalid launch (what=%d blocks=%d threads=%d iters=%d)", what, blocks, threads, iters);
+        return LDDMM_ERR_ARG;
+    }
+    LDDMM_TRY(check_device_ptr(out, "out"));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (what == 0)
+        probe_ffma_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999f, 1e-4f);
+    else
+        probe_ex2_kernel<<<blocks, threads, 0, st>>>(out, iters);
+    return cuda_check(cudaGetLastError(), "probe launch");
+}

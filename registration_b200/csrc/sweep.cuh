@@ -1,0 +1,140 @@
+// Generic tiled N-body sweep over (target block, source chunk) items.
+//
+// Each block owns BLOCK*R targets (R per thread, kept in registers) and one
+// chunk of the source range.  Source records (NS 16-byte words each, packed
+// structure-of-arrays in global memory, see Op::Src) are streamed through
+// shared memory in tiles of TILE records with a two-stage cp.async pipeline;
+// every warp reads the same record at the same time (shared-memory broadcast).
+// Per-target accumulators: FP32 partials over FOLD sources, folded into a
+// TwoSum-compensated (sum, err) pair (FP32 ops), or plain FP64 sums.
+// The block writes its per-target sums as doubles into the partial buffer
+//   part[(seg.part + chunk * seg.n_tgt + t) * Op::NOUT + c]
+// and a separate combine kernel adds the chunks in a fixed order, so results
+// do not depend on scheduling.
+#pragma once
+#include "common.cuh"
+
+namespace lddmm {
+
+template <class Op>
+__global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, const typename Op::Params P,
+                                                           double* __restrict__ part) {
+    using Real = typename Op::Real;
+    constexpr int BLOCK = Op::BLOCK, R = Op::R, TILE = Op::TILE, NS = Op::NS, NOUT = Op::NOUT;
+    constexpr int WORDS_PER_REC = NS;                  // 16-byte words per source record
+    constexpr int WORDS_PER_TILE = WORDS_PER_REC * TILE;
+    static_assert(WORDS_PER_TILE % BLOCK == 0, "tile must split evenly over the block");
+    __shared__ __align__(16) float4 smem[2][WORDS_PER_TILE];
+
+    const int item = blockIdx.x;
+    const SegDesc sg = find_segment(grid, item);
+    const int local = item - sg.item0;
+    const int tb = local % sg.n_tb;
+    const int chunk = local / sg.n_tb;
+    const int tile_lo = (int)(((long long)chunk * sg.n_src_tiles) / sg.split);
+    const int tile_hi = (int)(((long long)(chunk + 1) * sg.n_src_tiles) / sg.split);
+
+    // targets owned by this thread: t = tb*BLOCK*R + r*BLOCK + threadIdx.x (rows are padded)
+    typename Op::Tgt tg[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        long long row = sg.tgt + (long long)tb * BLOCK * R + r * BLOCK + threadIdx.x;
+        Op::load_target(P, row, tg[r]);
+    }
+    typename Op::Acc acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r].zero();
+
+    // global source words: Op lays a record out as NS planes of float4 words,
+    // plane p of record j at P.src4[p * P.src_stride + j]
+    auto load_tile = [&](int tile, int stage) {
+        const long long rec0 = sg.src + (long long)tile * TILE;
+#pragma unroll
+        for (int w = threadIdx.x; w < WORDS_PER_TILE; w += BLOCK) {
+            const int plane = w / TILE;
+            const int j = w - plane * TILE;
+            cp_async16(&smem[stage][w], P.src4 + (long long)plane * P.src_stride + rec0 + j);
+        }
+        cp_async_commit();
+    };
+
+    if (tile_lo < tile_hi) load_tile(tile_lo, 0);
+    for (int tile = tile_lo; tile < tile_hi; ++tile) {
+        const int stage = (tile - tile_lo) & 1;
+        if (tile + 1 < tile_hi) {
+            load_tile(tile + 1, stage ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float4* S = smem[stage];
+#pragma unroll 1
+        for (int j0 = 0; j0 < TILE; j0 += Op::FOLD) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r].begin_fold();
+#pragma unroll 4
+            for (int j = j0; j < j0 + Op::FOLD; ++j) {
+                typename Op::Src s;
+                Op::load_source(S, j, s);
+#pragma unroll
+                for (int r = 0; r < R; ++r) Op::pair(P, tg[r], s, acc[r]);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r].end_fold();
+        }
+        __syncthreads();
+    }
+
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = tb * BLOCK * R + r * BLOCK + threadIdx.x;
+        if (t < sg.n_tgt) {
+            double* dst = part + (sg.part + (long long)chunk * sg.n_tgt + t) * NOUT;
+#pragma unroll
+            for (int c = 0; c < NOUT; ++c) dst[c] = acc[r].value(c);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Accumulators
+// ---------------------------------------------------------------------------
+// FP32 partial over FOLD sources + TwoSum-compensated running sum.
+template <int N>
+struct AccF32C {
+    float p[N], s[N], e[N];
+    LDDMM_D void zero() {
+#pragma unroll
+        for (int c = 0; c < N; ++c) s[c] = e[c] = 0.f;
+    }
+    LDDMM_D void begin_fold() {
+#pragma unroll
+        for (int c = 0; c < N; ++c) p[c] = 0.f;
+    }
+    LDDMM_D void end_fold() {
+#pragma unroll
+        for (int c = 0; c < N; ++c) two_sum_acc(s[c], e[c], p[c]);
+    }
+    LDDMM_D void add(int c, float v) { p[c] += v; }
+    LDDMM_D void fma(int c, float a, float b) { p[c] = fmaf(a, b, p[c]); }
+    LDDMM_D double value(int c) const { return (double)s[c] + (double)e[c]; }
+};
+
+// Plain FP64 accumulation (the uncompensated FP64 comparator path).
+template <int N>
+struct AccF64 {
+    double s[N];
+    LDDMM_D void zero() {
+#pragma unroll
+        for (int c = 0; c < N; ++c) s[c] = 0.0;
+    }
+    LDDMM_D void begin_fold() {}
+    LDDMM_D void end_fold() {}
+    LDDMM_D void add(int c, double v) { s[c] += v; }
+    LDDMM_D void fma(int c, double a, double b) { s[c] = fma_rn(a, b, s[c]); }
+    LDDMM_D double value(int c) const { return s[c]; }
+    static LDDMM_D double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+};
+
+}  // namespace lddmm

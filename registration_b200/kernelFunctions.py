@@ -1,0 +1,149 @@
+"""Kernel API with the signatures of py-lddmm/kernelFunctions.py (KernelSpec,
+Kernel.applyK / applyDiffKT / applyDiffKmat ...), computed by the CUDA library.
+
+Drop-in rules kept from the reference:
+  * ``KernelSpec(name, affine, sigma, order, w1, w2, dim, center, weight)``:
+    'gauss' forces order 10, 'laplacian' orders above 4 become 3, any other
+    name means "no kernel" (kernelFunctions.py:238-268);
+  * ``applyK(x, a, firstVar=None)``: x are the sources, firstVar the targets
+    (x itself when None) (kernelFunctions.py:310-330);
+  * ``weight`` only scales ``precompute`` (dense matrices), never applyK
+    (kernelFunctions.py:285-298);
+  * outputs are fresh float64 arrays: numpy in -> numpy out; CUDA tensors in ->
+    CUDA tensors out (stays on the device).
+Only affine='none' is provided (affine kernel parts are outside the hot path).
+
+Extra keyword: ``precision`` = 'fp32c' (default: FP32 pair arithmetic with
+compensated accumulation, FP64 results) or 'fp64' (plain FP64 on the GPU).
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from .device import output_like, ptr, require_cuda, stream_handle, to_dev, workspace
+
+PRECISIONS = ("fp32c", "fp64")
+
+
+def _suffix(precision):
+    if precision not in PRECISIONS:
+        raise ValueError("precision must be one of %s" % (PRECISIONS,))
+    return "f32c" if precision == "fp32c" else "f64"
+
+
+class KernelSpec:
+    """Kernel parameters (kernelFunctions.py:238-280)."""
+
+    def __init__(self, name='gauss', affine='none', sigma=6.5, order=10, w1=1.0, w2=1.0, dim=3, center=(0, 0, 0),
+                 weight=1.0, precision='fp32c'):
+        self.name = name
+        self.sigma = sigma
+        self.order = order
+        self.weight = weight
+        self.w1 = w1
+        self.w2 = w2
+        self.constant_plane = False
+        self.center = np.array(center)
+        self.affine_basis = []
+        self.dim = dim
+        self.precomp = []
+        self._hold = False
+        self._state = False
+        self.affine = affine
+        self.precision = precision
+        _suffix(precision)
+        if name == 'laplacian':
+            if self.order > 4:
+                self.order = 3
+            self.par = [sigma, self.order]
+        elif name == 'gauss':
+            self.order = 10
+            self.par = [sigma]
+        else:
+            self.name = 'none'
+            self.par = []
+        if affine not in ('none', None):
+            raise NotImplementedError("affine kernel components are not part of this library (affine='none' only)")
+
+
+class Kernel(KernelSpec):
+    """Kernel with the apply* methods of kernelFunctions.py:284-530."""
+
+    # hold/release/reset keep the reference's state machine (kernelFunctions.py:300-307);
+    # no dense matrix is cached, so they have no numerical effect.
+    def hold(self):
+        self._state = self._hold
+        self._hold = True
+
+    def release(self):
+        self._state = False
+        self._hold = False
+
+    def reset(self):
+        self._hold = self._state
+
+    # ---- kernel sums -----------------------------------------------------
+    def applyK(self, x, a, firstVar=None, grid=None, matrixWeights=False):
+        """K(x, x) a, or K(firstVar, x) a (kernelFunctions.py:310-369)."""
+        if matrixWeights:
+            return self._applykmat(x, a, firstVar)
+        require_cuda()
+        src = to_dev(x)
+        w = to_dev(a)
+        tgt = src if firstVar is None else to_dev(firstVar)
+        if w.dim() != 2 or w.shape[0] != src.shape[0]:
+            raise ValueError("applyK: a must be (N, dimb) with N = x.shape[0]")
+        n, m, d, dimb = tgt.shape[0], src.shape[0], src.shape[1], w.shape[1]
+        if tgt.shape[1] != d:
+            raise ValueError("applyK: firstVar and x have different dimensions")
+        if self.name == 'none':
+            return output_like(x, torch.zeros((n, dimb), dtype=torch.float64, device=src.device))
+        f = torch.empty((n, dimb), dtype=torch.float64, device=src.device)
+        sfx = _suffix(self.precision)
+        wsb = _lib.query("lddmm_applyk_%s_workspace" % sfx, n, m, d, dimb)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_applyk_" + sfx, ptr(tgt), n, ptr(src), m, ptr(w), d, dimb, float(self.sigma),
+                  int(self.order), ptr(f), ptr(ws), wsb, stream_handle())
+        return output_like(x, f)
+
+    def applyDiffKT(self, x, a1, a2, firstVar=None):
+        """sum_l grad_1 [a1_k . K(y_k, x_l) a2_l] (kernelFunctions.py:412-449)."""
+        require_cuda()
+        src = to_dev(x)
+        tgt = src if firstVar is None else to_dev(firstVar)
+        A1 = _stack(a1)
+        A2 = _stack(a2)
+        if A1.dim() != 3 or A2.dim() != 3 or A1.shape[0] != A2.shape[0] or A1.shape[2] != A2.shape[2]:
+            raise ValueError("applyDiffKT: a1, a2 must be (na, N, dimb) with matching na and dimb")
+        na, dimb = A1.shape[0], A1.shape[2]
+        n, m, d = tgt.shape[0], src.shape[0], src.shape[1]
+        if A1.shape[1] != n or A2.shape[1] != m:
+            raise ValueError("applyDiffKT: a1 must cover the targets and a2 the sources")
+        if self.name == 'none':
+            return output_like(x, torch.zeros((n, d), dtype=torch.float64, device=src.device))
+        f = torch.empty((n, d), dtype=torch.float64, device=src.device)
+        sfx = _suffix(self.precision)
+        if na * dimb > 12:
+            # linear in the (i, c) terms: accumulate groups of whole momenta
+            step = max(1, 12 // dimb)
+            acc = None
+            for i0 in range(0, na, step):
+                part = self.applyDiffKT(src, A1[i0:i0 + step], A2[i0:i0 + step],
+                                        firstVar=None if firstVar is None else tgt)
+                acc = part if acc is None else acc + part
+            return output_like(x, acc)
+        wsb = _lib.query("lddmm_applykdifft_%s_workspace" % sfx, n, m, na, d, dimb)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_applykdifft_" + sfx, ptr(tgt), n, ptr(src), m, ptr(A1), ptr(A2), na, d, dimb,
+                  float(self.sigma), int(self.order), ptr(f), ptr(ws), wsb, stream_handle())
+        return output_like(x, f)
+
+    def _applykmat(self, x, a, firstVar):
+        raise NotImplementedError("matrixWeights=True is provided by the fused varifold kernels")
+
+
+def _stack(a):
+    if isinstance(a, (list, tuple)):
+        return torch.stack([to_dev(t) for t in a]).contiguous()
+    t = to_dev(a)
+    return t
