@@ -86,6 +86,100 @@ LDDMM_API int lddmm_applykdifft_f64(const double* x, int64_t n, const double* y,
                           const double* a2, int na, int d, int dimb, double sigma, int order, double* f,
                           void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
+/* ---- divergence: Kernel.applyDivergence -------------------------------------
+ * Replaces the dense numpy applyDivergence (py-lddmm/kernelFunctions.py:510-530,
+ * used by landmarkDirectEvolutionEuler(withJacobian=True)), without the
+ * kernel weight factor (the caller multiplies by KernelSpec.weight):
+ *   f[k] = sum_l K'(x_k, y_l) 2 <x_k - y_l, a_l>
+ * x (n, d) targets, y (m, d) sources, a (m, d), f (n). */
+LDDMM_API size_t lddmm_applydiv_f32c_workspace(int64_t n, int64_t m, int d);
+LDDMM_API int lddmm_applydiv_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* a, int d,
+                                  double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                                  lddmm_stream_t stream);
+LDDMM_API size_t lddmm_applydiv_f64_workspace(int64_t n, int64_t m, int d);
+LDDMM_API int lddmm_applydiv_f64(const double* x, int64_t n, const double* y, int64_t m, const double* a, int d,
+                                 double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                                 lddmm_stream_t stream);
+
+/* ---- geodesic shooting: pointEvolution.landmarkDirectEvolutionEuler ----------
+ * Replaces the T-step Euler loop of py-lddmm/pointEvolution.py:666-730 (no
+ * affine part, no optional outputs):
+ *   xt[0] = x0,  xt[t+1] = xt[t] + dt K(xt[t], xt[t]) at[t],  dt = 1/T
+ * and, if energy != NULL, writes energy[0] = sum_t rw dt <at[t], K(xt[t]) at[t]>,
+ * the deformation cost of objectiveFunDef (py-lddmm/surfaceMatching.py:205-212,
+ * curveMatching.py:168-173), from the same kernel sums.
+ * x0 (n, d), at (T, n, d), xt (T+1, n, d); energy: one double on the device. */
+LDDMM_API size_t lddmm_shoot_f32c_workspace(int64_t n, int d, int T);
+LDDMM_API int lddmm_shoot_f32c(const double* x0, int64_t n, int d, const double* at, int T, double sigma, int order,
+                               double regweight, double* xt, double* energy, void* workspace, size_t workspace_bytes,
+                               lddmm_stream_t stream);
+LDDMM_API size_t lddmm_shoot_f64_workspace(int64_t n, int d, int T);
+LDDMM_API int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* at, int T, double sigma, int order,
+                              double regweight, double* xt, double* energy, void* workspace, size_t workspace_bytes,
+                              lddmm_stream_t stream);
+
+/* ---- Hamiltonian adjoint: landmarkHamiltonianCovector / Gradient --------------
+ * Replaces the backward loop of py-lddmm/pointEvolution.py:735-765 and the
+ * gradient of :793-817 (no affine part), given the trajectory xt:
+ *   pxt[T] = px1,
+ *   pxt[t] = pxt[t+1] + dt applyDiffKT(xt[t], [pxt[t+1], at[t], -2 rw at[t]],
+ *                                             [at[t], pxt[t+1], at[t]]),
+ *   dat[t] = 2 rw at[t] - pxt[t+1]          (dat may be NULL)
+ * xt (T+1, n, d), at (T, n, d), px1 (n, d), pxt (T+1, n, d), dat (T, n, d). */
+LDDMM_API size_t lddmm_covector_f32c_workspace(int64_t n, int d, int T);
+LDDMM_API int lddmm_covector_f32c(const double* xt, int64_t n, int d, const double* at, int T, const double* px1,
+                                  double sigma, int order, double regweight, double* pxt, double* dat, void* workspace,
+                                  size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API size_t lddmm_covector_f64_workspace(int64_t n, int d, int T);
+LDDMM_API int lddmm_covector_f64(const double* xt, int64_t n, int d, const double* at, int T, const double* px1,
+                                 double sigma, int order, double regweight, double* pxt, double* dat, void* workspace,
+                                 size_t workspace_bytes, lddmm_stream_t stream);
+
+/* ---- EPDiff shooting: pointEvolution.landmarkEPDiff ---------------------------
+ * Replaces py-lddmm/pointEvolution.py:599-658 (no affine / optional outputs):
+ *   xt[k+1] = xt[k] + dt K(xt[k]) at[k],
+ *   at[k+1] = at[k] - dt applyDiffKT(xt[k], [at[k]], [at[k]])   (k < T-1)
+ * x0, a0 (n, d), xt (T+1, n, d), at (T, n, d). */
+LDDMM_API size_t lddmm_epdiff_f32c_workspace(int64_t n, int d, int T);
+LDDMM_API int lddmm_epdiff_f32c(const double* x0, int64_t n, int d, const double* a0, int T, double sigma, int order,
+                                double* xt, double* at, void* workspace, size_t workspace_bytes,
+                                lddmm_stream_t stream);
+LDDMM_API size_t lddmm_epdiff_f64_workspace(int64_t n, int d, int T);
+LDDMM_API int lddmm_epdiff_f64(const double* x0, int64_t n, int d, const double* a0, int T, double sigma, int order,
+                               double* xt, double* at, void* workspace, size_t workspace_bytes,
+                               lddmm_stream_t stream);
+
+/* ---- data attachment: surfaces / curves current, measure, varifold ------------
+ * Replaces surfaces.{current,measure,varifold}Norm{0,Def,Gradient}
+ * (py-lddmm/surfaces.py:1009-1276) and curves.{current,measure}Norm{0,Def,Gradient}
+ * (py-lddmm/curves.py:539-703) -- the fun_obj0 / fun_obj / fun_objGrad plug-in
+ * triple of SurfaceMatchingParam.errorType (surfaceMatching.py:29-40).
+ *   cell_size   3: triangles (d = 3), 2: edges (d = 2 or 3)
+ *   norm        0 current, 1 measure, 2 varifold (triangles only)
+ *   vertices (nv, d) and cells (nc, cell_size) int64 of the deformed shape S1;
+ *   tgt_centers / tgt_vectors (nc2, d): centres and surfels/tangents of the
+ *   target shape S2 (nc2 = 0 for Norm0 of S1);
+ *   eps1 / eps2: the constant under the square root of the cell weights of S1
+ *   and S2 (1e-10 in the reference, 0 in curves.measureNorm0);
+ *   energy (if not NULL): <S1,S1> - 2 <S1,S2>  (NormDef; Norm0 with nc2 = 0);
+ *   px (if not NULL): the gradient of |S1 - S2|^2 w.r.t. the vertices (nv, d)
+ *   (NormGradient); it needs the vertex -> (cell, corner) incidence in CSR form:
+ *   vertex_ptr (nv+1), vertex_idx (nc*cell_size) with entries cell*cell_size+corner. */
+LDDMM_API size_t lddmm_dataterm_f32c_workspace(int cell_size, int norm, int64_t nv, int d, int64_t nc, int64_t nc2,
+                                               int order, int want_energy, int want_grad);
+LDDMM_API int lddmm_dataterm_f32c(int cell_size, int norm, const double* vertices, int64_t nv, int d,
+                                  const int64_t* cells, int64_t nc, const double* tgt_centers,
+                                  const double* tgt_vectors, int64_t nc2, double sigma, int order, double eps1,
+                                  double eps2, double* energy, const int64_t* vertex_ptr, const int64_t* vertex_idx,
+                                  double* px, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API size_t lddmm_dataterm_f64_workspace(int cell_size, int norm, int64_t nv, int d, int64_t nc, int64_t nc2,
+                                              int order, int want_energy, int want_grad);
+LDDMM_API int lddmm_dataterm_f64(int cell_size, int norm, const double* vertices, int64_t nv, int d,
+                                 const int64_t* cells, int64_t nc, const double* tgt_centers,
+                                 const double* tgt_vectors, int64_t nc2, double sigma, int order, double eps1,
+                                 double eps2, double* energy, const int64_t* vertex_ptr, const int64_t* vertex_idx,
+                                 double* px, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+
 /* ---- diagnostics ------------------------------------------------------------
  * No counterpart in the reference.  Launches `blocks` x `threads` threads that
  * each issue 8*iters FP32 FMAs (what = 0) or 8*iters MUFU ex2 (what = 1) and

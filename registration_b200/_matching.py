@@ -1,0 +1,191 @@
+"""Device-resident implementation of the matching-problem protocol shared by
+SurfaceMatching (py-lddmm/surfaceMatching.py:74-486) and CurveMatching
+(py-lddmm/curveMatching.py:58-354): objectiveFunDef / objectiveFun /
+updateTry / getGradient / dotProduct / acceptVarTry / endOfIteration.
+
+Momenta, trajectory, directions and shapes stay on the GPU (FP64 storage);
+every objective value and dot product is reduced in FP64 on the device and
+read back as one host double, which is what the line search compares.
+
+Two reuses that do not change any value: the trajectory of an accepted trial
+step is kept instead of re-shooting it in endOfIteration, and getGradient
+runs the adjoint on that stored trajectory instead of re-shooting inside
+landmarkHamiltonianGradient (the shots are deterministic, so they would be
+bit-identical).
+"""
+import logging
+
+import numpy as np
+import torch
+
+from . import _dataterm as _dt
+from . import pointEvolution as evol
+from .device import require_cuda, to_dev
+
+
+class Direction:
+    def __init__(self):
+        self.diff = []
+        self.aff = []
+        self.initx = []
+
+
+class DeviceMatching:
+    """Subclasses set: fv0, fv1 (shapes), param, norm_name, tgt_vectors_attr."""
+
+    def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric):
+        require_cuda()
+        if affine not in ('none', None):
+            raise NotImplementedError("affine registration components are not provided (affine='none' only)")
+        if symmetric:
+            raise NotImplementedError("symmetric matching is not provided")
+        self.maxIter = maxIter
+        self.verb = verb
+        self.testGradient = testGradient
+        self.regweight = regWeight
+        self.affine = 'none'
+        self.affineDim = 0
+        self.symmetric = False
+        self.iter = 0
+        self.Tsize = int(round(1.0 / self.param.timeStep))
+        self.x0 = to_dev(self.fv0.vertices)
+        self.npt, self.dim = self.x0.shape
+        dev = self.x0.device
+        self.at = torch.zeros((self.Tsize, self.npt, self.dim), dtype=torch.float64, device=dev)
+        self.atTry = self.at.clone()
+        self.Afft = np.zeros((self.Tsize, 0))
+        self.AfftTry = self.Afft
+        self.xt = self.x0.unsqueeze(0).repeat(self.Tsize + 1, 1, 1)
+        self.xtTry = None
+        self.obj = None
+        self.objTry = None
+        self.gradCoeff = self.npt
+        self._dshape = self.fv0.device_shape()
+        self._tc = to_dev(self.fv1.centers)
+        self._tv = to_dev(getattr(self.fv1, self.tgt_vectors_attr))
+        self.fvDef.updateVertices(self.x0)
+        self._fast_data = self._our_norm_functions()
+
+    # -- data term ------------------------------------------------------------
+    def _our_norm_functions(self):
+        """True when param's (fun_obj0, fun_obj, fun_objGrad) are this library's
+        own norms, so the device path can be used directly."""
+        mod = self.norm_module
+        name = getattr(self.param, 'errorType', None)
+        if name not in ('current', 'measure', 'varifold'):
+            return False
+        want = (getattr(mod, name + 'Norm0', None), getattr(mod, name + 'NormDef', None),
+                getattr(mod, name + 'NormGradient', None))
+        return (self.param.fun_obj0, self.param.fun_obj, self.param.fun_objGrad) == want
+
+    def _data_energy(self, vertices):
+        """fun_obj(fvDef, fv1, KparDist) / sigmaError^2 as a device scalar."""
+        if self._fast_data:
+            e, _ = _dt.dataterm(self.param.errorType, vertices, self._dshape, self._tc, self._tv,
+                                self.param.KparDist, energy=True, grad=False)
+            return e / (self.param.sigmaError ** 2)
+        ff = self.shape_copy(self.fvDef)
+        ff.updateVertices(vertices)
+        return torch.tensor(self.param.fun_obj(ff, self.fv1, self.param.KparDist) / self.param.sigmaError ** 2,
+                            dtype=torch.float64, device=self.x0.device)
+
+    def dataTerm(self, _fvDef, _fvInit=None):
+        return float(self._data_energy(to_dev(_fvDef.vertices)))
+
+    def endPointGradient(self):
+        if self._fast_data:
+            _, px = _dt.dataterm(self.param.errorType, self.xt[-1], self._dshape, self._tc, self._tv,
+                                 self.param.KparDist, energy=False, grad=True)
+        else:
+            px = to_dev(self.param.fun_objGrad(self.fvDef, self.fv1, self.param.KparDist))
+        return px / self.param.sigmaError ** 2
+
+    # -- objective --------------------------------------------------------------
+    def objectiveFunDef(self, at, Afft=None, withTrajectory=False, withJacobian=False, x0=None):
+        """Deformation cost sum_t rw dt <a_t, K(x_t) a_t> (surfaceMatching.py:187-221)."""
+        x0 = self.x0 if x0 is None else to_dev(x0)
+        xt, e = evol.shoot(x0, to_dev(at), self.param.KparDiff, regweight=self.regweight, with_energy=True)
+        obj = float(e)
+        if withJacobian:
+            _, Jt = evol.landmarkDirectEvolutionEuler(x0, to_dev(at), self.param.KparDiff, withJacobian=True)
+            return obj, xt, Jt
+        if withTrajectory:
+            return obj, xt
+        return obj
+
+    def objectiveFun(self):
+        """(surfaceMatching.py:233-250)"""
+        if self.obj is None:
+            self.obj0 = self.param.fun_obj0(self.fv1, self.param.KparDist) / (self.param.sigmaError ** 2)
+            xt, e = evol.shoot(self.x0, self.at, self.param.KparDiff, regweight=self.regweight, with_energy=True)
+            self.xt = xt
+            self.fvDef.updateVertices(xt[-1])
+            self.obj = float(e + self._data_energy(xt[-1])) + self.obj0
+        return self.obj
+
+    def getVariable(self):
+        return [self.at, self.Afft]
+
+    def updateTry(self, dir, eps, objRef=None):
+        """(surfaceMatching.py:255-289); NaN objectives return 1e500."""
+        atTry = self.at - eps * dir.diff
+        xt, e = evol.shoot(self.x0, atTry, self.param.KparDiff, regweight=self.regweight, with_energy=True)
+        objTry = self.obj0 + float(e + self._data_energy(xt[-1]))
+        if np.isnan(objTry):
+            logging.info('Warning: nan in updateTry')
+            return 1e500
+        if (objRef is None) or (objTry < objRef):
+            self.atTry = atTry
+            self.objTry = objTry
+            self.xtTry = xt
+        return objTry
+
+    def getGradient(self, coeff=1.0):
+        """(surfaceMatching.py:301-327): grd.diff = (2 rw a - p_{t+1}) / (coeff T)."""
+        px1 = -self.endPointGradient()
+        _, dat = evol.covector(self.xt, self.at, px1, self.param.KparDiff, self.regweight, with_dat=True)
+        grd = Direction()
+        grd.diff = dat / (coeff * self.Tsize)
+        grd.aff = np.zeros(self.Afft.shape)
+        return grd
+
+    def addProd(self, dir1, dir2, beta):
+        d = Direction()
+        d.diff = dir1.diff + beta * dir2.diff
+        d.aff = dir1.aff
+        return d
+
+    def copyDir(self, dir0):
+        d = Direction()
+        d.diff = dir0.diff.clone()
+        d.aff = np.copy(dir0.aff)
+        return d
+
+    def randomDir(self):
+        d = Direction()
+        d.diff = torch.randn((self.Tsize, self.npt, self.dim), dtype=torch.float64, device=self.x0.device)
+        d.aff = np.zeros(self.Afft.shape)
+        return d
+
+    def dotProduct(self, g1, g2):
+        """sum_t <g2_t, K(x_t) g1_t> (surfaceMatching.py:353-377), FP64 on the device."""
+        acc = torch.zeros(len(g2), dtype=torch.float64, device=self.x0.device)
+        K = self.param.KparDiff
+        for t in range(self.Tsize):
+            u = K.applyK(self.xt[t], g1.diff[t])
+            for ll, gr in enumerate(g2):
+                acc[ll] += (gr.diff[t] * u).sum()
+        return acc.cpu().numpy()
+
+    def acceptVarTry(self):
+        self.obj = self.objTry
+        self.at = self.atTry.clone()
+        if self.xtTry is not None:
+            self.xt = self.xtTry
+
+    def endOfIteration(self):
+        self.iter += 1
+        self.fvDef.updateVertices(self.xt[-1])
+
+    def endOptim(self):
+        pass

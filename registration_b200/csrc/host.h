@@ -42,7 +42,9 @@ DeviceInfo device_info();
 int occupancy_blocks(const void* kernel, int block, size_t dyn_smem = 0);
 
 // Number of source chunks for a sweep: enough items (target blocks x chunks)
-// for about 8 waves of resident blocks, at least 2 source tiles per chunk.
+// for about 8 waves of `slots` resident blocks, at least 2 source tiles per
+// chunk.  `slots` is taken as 8 blocks per SM for every operator, so the split
+// (and the workspace) depends only on the shape and the SM count.
 inline int choose_split(int n_tb, int n_src_tiles, int slots) {
     if (n_tb <= 0 || n_src_tiles <= 0) return 1;
     long long want = (8LL * slots + n_tb - 1) / n_tb;

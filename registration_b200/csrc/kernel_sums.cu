@@ -30,6 +30,7 @@ int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) 
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * DIMB);
+    double* center = ws.take<double>(4);
     if (ws.measuring()) return LDDMM_OK;
     if (ws.overflow()) {
         set_error("workspace too small: need %zu bytes, got %zu", ws.off, ws.cap);
@@ -43,8 +44,11 @@ int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) 
     P.tgt_stride = pl.n_tpad;
     for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
     for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
-    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, tgt, pl.n_tpad, pl.n_tpad);
-    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, src, pl.m_pad, pl.m_pad);
+    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
+                                                                  pl.n_tpad);
+    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
+                                                                 pl.m_pad);
     Gather g{};
     g.src = a.beta;
     g.row_stride = a.dimb;
@@ -163,6 +167,7 @@ int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
     float4* tgt = ws.take<float4>((size_t)Op::NS * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * D);
+    double* center = ws.take<double>(4);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     typename Op::Params P{};
@@ -172,8 +177,11 @@ int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
     P.tgt_stride = pl.n_tpad;
     for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
     for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
-    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, tgt, pl.n_tpad, pl.n_tpad);
-    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, src, pl.m_pad, pl.m_pad);
+    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
+                                                                  pl.n_tpad);
+    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
+                                                                 pl.m_pad);
     // u_k / v_l: value w = c*na + i  <->  a[i, row, c]  (the Fortran sum order)
     Gather gu{}, gv{};
     gu.src = a.a1;
@@ -268,6 +276,83 @@ int difft_entry(const DiffKTArgs& a, void* wsp, size_t wsb, cudaStream_t st) {
     return difft_run<Real>(a, ws, st);
 }
 
+// ---------------------------------------------------------------------------
+// applyDivergence
+// ---------------------------------------------------------------------------
+template <class Real, int KIND, int DEG, int D>
+int div_impl(const ApplyKArgs& a, Workspace& ws, cudaStream_t st) {
+    using Op = OpDivergence<Real, KIND, DEG, D>;
+    const SinglePlan pl = plan_single<Op>(a.n, a.m);
+    float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
+    float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
+    double* part = ws.take<double>((size_t)pl.split * a.n);
+    double* center = ws.take<double>(4);
+    if (ws.measuring()) return LDDMM_OK;
+    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
+    typename Op::Params P{};
+    P.src4 = src;
+    P.src_stride = pl.m_pad;
+    P.tgt4 = tgt;
+    P.tgt_stride = pl.n_tpad;
+    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
+    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
+                                                                  pl.n_tpad);
+    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
+                                                                 pl.m_pad);
+    Gather g{};
+    g.src = a.beta;
+    g.row_stride = a.d;
+    g.nvals = a.d;
+    for (int c = 0; c < a.d; ++c) g.off[c] = c;
+    g.mult = 1.0;  // K' 2 <x-y, a> = dscale * F * <x'-y', a>
+    pack_values_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(g, a.m, src, pl.m_pad, pl.m_pad, Op::PP);
+    LDDMM_TRY(launch_single<Op>(pl, a.n, P, part, st));
+    combine_kernel<<<grid_for(a.n), 256, 0, st>>>(part, a.n, 1, pl.split, ks.dscale, a.f, 1, 0);
+    return cuda_check(cudaGetLastError(), "applydiv");
+}
+
+template <class Real>
+int div_run(const ApplyKArgs& a, Workspace& ws, cudaStream_t st) {
+    return dispatch_kind_q(a.order, [&](auto kind, auto deg) {
+        return dispatch_d(a.d, [&](auto D) {
+            return div_impl<Real, decltype(kind)::value, decltype(deg)::value, decltype(D)::value>(a, ws, st);
+        });
+    });
+}
+
+template <class Real>
+size_t div_ws(int64_t n, int64_t m, int d) {
+    if (n <= 0 || m <= 0 || d < 1 || d > 3) return 0;
+    ApplyKArgs a{nullptr, n, nullptr, m, nullptr, d, d, 1.0, 10, nullptr};
+    Workspace ws;
+    div_run<Real>(a, ws, 0);
+    return ws.off + 256;
+}
+
+template <class Real>
+int div_entry(const ApplyKArgs& a, void* wsp, size_t wsb, cudaStream_t st) {
+    LDDMM_TRY(applyk_validate(a));
+    if (a.order == 0) {
+        set_error("applydiv: the order-0 Laplacian kernel is not differentiable");
+        return LDDMM_ERR_ARG;
+    }
+    if (a.n == 0) return LDDMM_OK;
+    if (a.m == 0) return cuda_check(cudaMemsetAsync(a.f, 0, sizeof(double) * a.n, st), "applydiv memset");
+    Workspace meas;
+    div_run<Real>(a, meas, st);
+    if (wsp == nullptr || meas.off > wsb) {
+        set_error("applydiv: workspace too small: need %zu bytes, got %zu", meas.off, wsb);
+        return LDDMM_ERR_WORKSPACE;
+    }
+    LDDMM_TRY(check_device_ptr(wsp, "workspace"));
+    Workspace ws;
+    ws.base = static_cast<char*>(wsp);
+    ws.cap = wsb;
+    return div_run<Real>(a, ws, st);
+}
+
 }  // namespace lddmm
 
 using namespace lddmm;
@@ -310,6 +395,21 @@ int lddmm_applykdifft_f64(const double* x, int64_t n, const double* y, int64_t m
                           void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
     DiffKTArgs a{x, n, y, m, a1, a2, na, d, dimb, sigma, order, f};
     return difft_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+size_t lddmm_applydiv_f32c_workspace(int64_t n, int64_t m, int d) { return div_ws<float>(n, m, d); }
+size_t lddmm_applydiv_f64_workspace(int64_t n, int64_t m, int d) { return div_ws<double>(n, m, d); }
+
+int lddmm_applydiv_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* a, int d, double sigma,
+                        int order, double* f, void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
+    ApplyKArgs q{x, n, y, m, a, d, d, sigma, order, f};
+    return div_entry<float>(q, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int lddmm_applydiv_f64(const double* x, int64_t n, const double* y, int64_t m, const double* a, int d, double sigma,
+                       int order, double* f, void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
+    ApplyKArgs q{x, n, y, m, a, d, d, sigma, order, f};
+    return div_entry<double>(q, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -200,4 +200,48 @@ struct OpDiffKT {
     }
 };
 
+// ---------------------------------------------------------------------------
+// div_k = sum_l K'(x_k,y_l) 2 <x_k - y_l, a_l>      (up to the combine scale)
+// py-lddmm/kernelFunctions.py:510-530 (applyDivergence)
+// ---------------------------------------------------------------------------
+template <class Real_, int KIND, int DEG, int D>
+struct OpDivergence {
+    using Real = Real_;
+    static constexpr bool F32 = sizeof(Real) == 4;
+    static constexpr int BLOCK = 128;
+    static constexpr int R = 4;
+    static constexpr int TILE = 128;
+    static constexpr int FOLD = F32 ? 32 : TILE;
+    static constexpr int PP = PointPlanes<Real>::N;
+    static constexpr int WP = (D + Traits<Real>::PER_WORD - 1) / Traits<Real>::PER_WORD;
+    static constexpr int NS = PP + WP;
+    static constexpr int NOUT = 1;
+    using Params = KernelParamsBase<Real>;
+    using Acc = typename AccFor<Real>::template type<1>;
+    struct Tgt {
+        Real x[D];
+    };
+    struct Src {
+        Real y[D];
+        Real a[D];
+    };
+    static LDDMM_D void load_target(const Params& P, long long row, Tgt& t) {
+        load_vals<Real, D>(P.tgt4, P.tgt_stride, row, 0, t.x);
+    }
+    static LDDMM_D void load_source(const float4* S, int j, Src& s) {
+        load_vals_smem<Real, D, TILE>(S, j, 0, s.y);
+        load_vals_smem<Real, D, TILE>(S, j, PP, s.a);
+    }
+    static LDDMM_D void pair(const Params& P, const Tgt& t, const Src& s, Acc& acc) {
+        Real r2 = 0, dot = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            const Real dj = t.x[j] - s.y[j];
+            r2 = j == 0 ? dj * dj : r2 + dj * dj;
+            dot = j == 0 ? dj * s.a[j] : dot + dj * s.a[j];
+        }
+        acc.fma(0, kdiff<Real, KIND, DEG>(P.pq, r2), dot);
+    }
+};
+
 }  // namespace lddmm

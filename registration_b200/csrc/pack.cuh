@@ -6,16 +6,49 @@
 
 namespace lddmm {
 
-// Points: value j of row i is x[i*d + j] * scale (zero for j >= d or i >= n).
+// Centre of the bounding box of x (n, d) and y (m, d): center[0..d).  The
+// kernels are translation invariant, and packing coordinates relative to this
+// centre halves the magnitude (and so the FP32 rounding error) of the packed
+// coordinates.  One block; min/max do not depend on the reduction order.
+static __global__ void bbox_center_kernel(const double* __restrict__ x, long long n, const double* __restrict__ y,
+                                          long long m, int d, double* __restrict__ center) {
+    __shared__ double lo[3][256], hi[3][256];
+    double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
+    for (long long i = threadIdx.x; i < n + m; i += blockDim.x) {
+        const double* p = i < n ? x + i * d : y + (i - n) * d;
+        for (int j = 0; j < d; ++j) {
+            l[j] = fmin(l[j], p[j]);
+            h[j] = fmax(h[j], p[j]);
+        }
+    }
+    for (int j = 0; j < 3; ++j) {
+        lo[j][threadIdx.x] = l[j];
+        hi[j][threadIdx.x] = h[j];
+    }
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int j = 0; j < 3; ++j) {
+                lo[j][threadIdx.x] = fmin(lo[j][threadIdx.x], lo[j][threadIdx.x + s]);
+                hi[j][threadIdx.x] = fmax(hi[j][threadIdx.x], hi[j][threadIdx.x + s]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int j = 0; j < 3; ++j) center[j] = j < d && n + m > 0 ? 0.5 * (lo[j][0] + hi[j][0]) : 0.0;
+}
+
+// Points: value j of row i is (x[i*d + j] - center[j]) * scale (zero for j >= d or i >= n).
 // FP32: one float4 word per row in plane 0.  FP64: two double2 words (planes 0, 1).
 template <class Real>
 static __global__ void pack_points_kernel(const double* __restrict__ x, long long n, int d, double scale,
-                                   float4* __restrict__ out, long long stride, long long n_pad) {
+                                          const double* __restrict__ center, float4* __restrict__ out,
+                                          long long stride, long long n_pad) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_pad;
          i += (long long)gridDim.x * blockDim.x) {
         double v[4] = {0, 0, 0, 0};
         if (i < n)
-            for (int j = 0; j < d && j < 4; ++j) v[j] = x[i * d + j] * scale;
+            for (int j = 0; j < d && j < 4; ++j) v[j] = (x[i * d + j] - (center ? center[j] : 0.0)) * scale;
         if constexpr (sizeof(Real) == 4) {
             out[i] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
         } else {

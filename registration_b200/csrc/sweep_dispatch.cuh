@@ -12,11 +12,11 @@ namespace lddmm {
 template <int V>
 using IC = std::integral_constant<int, V>;
 
-// Blocks of this sweep that fit on the whole device at once.
+// Nominal resident blocks of a sweep on the whole device (8 per SM for every
+// operator, so plans and workspaces do not depend on register allocation).
 template <class Op>
 int sweep_slots() {
-    static const int occ = occupancy_blocks((const void*)sweep_kernel<Op>, Op::BLOCK);
-    return occ * device_info().sms;
+    return 8 * device_info().sms;
 }
 
 struct SinglePlan {

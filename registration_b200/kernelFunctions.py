@@ -138,6 +138,26 @@ class Kernel(KernelSpec):
                   float(self.sigma), int(self.order), ptr(f), ptr(ws), wsb, stream_handle())
         return output_like(x, f)
 
+    def applyDivergence(self, x, a, firstVar=None):
+        """sum_l div_1 K(y_k, x_l) a_l, times KernelSpec.weight as the dense
+        precompute path of the reference (kernelFunctions.py:509-530)."""
+        require_cuda()
+        src = to_dev(x)
+        w = to_dev(a)
+        tgt = src if firstVar is None else to_dev(firstVar)
+        n, m, d = tgt.shape[0], src.shape[0], src.shape[1]
+        if self.name == 'none':
+            return output_like(x, torch.zeros(n, dtype=torch.float64, device=src.device))
+        f = torch.empty(n, dtype=torch.float64, device=src.device)
+        sfx = _suffix(self.precision)
+        wsb = _lib.query("lddmm_applydiv_%s_workspace" % sfx, n, m, d)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_applydiv_" + sfx, ptr(tgt), n, ptr(src), m, ptr(w), d, float(self.sigma), int(self.order),
+                  ptr(f), ptr(ws), wsb, stream_handle())
+        if self.weight != 1.0:
+            f = f * self.weight
+        return output_like(x, f)
+
     def _applykmat(self, x, a, firstVar):
         raise NotImplementedError("matrixWeights=True is provided by the fused varifold kernels")
 

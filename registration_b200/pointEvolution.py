@@ -1,0 +1,151 @@
+"""Landmark evolution with the signatures of py-lddmm/pointEvolution.py, on the GPU.
+
+  landmarkDirectEvolutionEuler (pointEvolution.py:666-730)
+  landmarkEPDiff               (pointEvolution.py:599-658)
+  landmarkHamiltonianCovector  (pointEvolution.py:735-765)
+  landmarkHamiltonianGradient  (pointEvolution.py:793-817)
+
+The plain shot and the adjoint each run as one fused C-ABI call (one kernel
+sweep + one combine per time step).  The optional outputs of the direct
+evolution (withPointSet / withJacobian / withNormals) are evaluated step by
+step with the kernel-sum operators.  Affine parts: only the all-zero affine
+arguments that the matching code passes for affine='none' are accepted.
+
+numpy in -> numpy out; CUDA tensors in -> CUDA tensors out.
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from .device import is_device, output_like, ptr, require_cuda, stream_handle, to_dev, workspace
+from .kernelFunctions import _suffix
+
+
+def _check_affine(affine):
+    if affine is None:
+        return
+    for part in affine:
+        arr = part.detach().cpu().numpy() if isinstance(part, torch.Tensor) else np.asarray(part)
+        if arr.size and np.any(arr != 0):
+            raise NotImplementedError("non-zero affine components are not supported (affine='none' only)")
+
+
+def _kernel_args(K):
+    if K.name == 'none':
+        raise ValueError("a kernel is required")
+    return float(K.sigma), int(K.order), _suffix(K.precision)
+
+
+def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False):
+    """Device call: returns (xt, energy) with energy = sum_t rw dt <a_t, K(x_t) a_t> (a 0-d tensor) or None."""
+    require_cuda()
+    x0d = to_dev(x0)
+    atd = to_dev(at)
+    T, n, d = atd.shape
+    if x0d.shape != (n, d):
+        raise ValueError("x0 must be (N, dim) and at (T, N, dim)")
+    sigma, order, sfx = _kernel_args(KparDiff)
+    xt = torch.empty((T + 1, n, d), dtype=torch.float64, device=x0d.device)
+    energy = torch.empty((), dtype=torch.float64, device=x0d.device) if with_energy else None
+    wsb = _lib.query("lddmm_shoot_%s_workspace" % sfx, n, d, T)
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_shoot_" + sfx, ptr(x0d), n, d, ptr(atd), T, sigma, order, float(regweight), ptr(xt),
+              ptr(energy) if energy is not None else None, ptr(ws), wsb, stream_handle())
+    return xt, energy
+
+
+def covector(xt, at, px1, KparDiff, regweight, with_dat=True):
+    """Device call: returns (pxt, dat) given the trajectory xt (T+1, N, dim)."""
+    require_cuda()
+    xtd, atd, pxd = to_dev(xt), to_dev(at), to_dev(px1)
+    T, n, d = atd.shape
+    sigma, order, sfx = _kernel_args(KparDiff)
+    pxt = torch.empty((T + 1, n, d), dtype=torch.float64, device=xtd.device)
+    dat = torch.empty((T, n, d), dtype=torch.float64, device=xtd.device) if with_dat else None
+    wsb = _lib.query("lddmm_covector_%s_workspace" % sfx, n, d, T)
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_covector_" + sfx, ptr(xtd), n, d, ptr(atd), T, ptr(pxd), sigma, order, float(regweight),
+              ptr(pxt), ptr(dat) if dat is not None else None, ptr(ws), wsb, stream_handle())
+    return pxt, dat
+
+
+def landmarkDirectEvolutionEuler(x0, at, KparDiff, affine=None, withJacobian=False, withNormals=None,
+                                 withPointSet=None):
+    """Solves dx/dt = K(x,x) a(t) with x(0) = x0 (pointEvolution.py:662-730)."""
+    _check_affine(affine)
+    if withNormals is None and withPointSet is None and not withJacobian:
+        xt, _ = shoot(x0, at, KparDiff)
+        return output_like(x0, xt)
+    require_cuda()
+    x0d, atd = to_dev(x0), to_dev(at)
+    M = atd.shape[0] + 1
+    timeStep = 1.0 / (M - 1)
+    xt, _ = shoot(x0d, atd, KparDiff)
+    out = [xt]
+    if withPointSet is not None:
+        yt = torch.empty((M,) + tuple(to_dev(withPointSet).shape), dtype=torch.float64, device=x0d.device)
+        yt[0] = to_dev(withPointSet)
+        if withJacobian:
+            Jt = torch.zeros((M, yt.shape[1]), dtype=torch.float64, device=x0d.device)
+    elif withJacobian:
+        Jt = torch.zeros((M, atd.shape[1]), dtype=torch.float64, device=x0d.device)
+    if withNormals is not None:
+        nt = torch.empty_like(xt)
+        nt[0] = to_dev(withNormals)
+    for k in range(M - 1):
+        z, a = xt[k], atd[k]
+        if withPointSet is not None:
+            yt[k + 1] = yt[k] + timeStep * KparDiff.applyK(z, a, firstVar=yt[k])
+            if withJacobian:
+                Jt[k + 1] = Jt[k] + timeStep * KparDiff.applyDivergence(z, a, firstVar=yt[k])
+        elif withJacobian:
+            Jt[k + 1] = Jt[k] + timeStep * KparDiff.applyDivergence(z, a)
+        if withNormals is not None:
+            nt[k + 1] = nt[k] - timeStep * KparDiff.applyDiffKT(z, nt[k][None], a[None])
+    if withPointSet is not None:
+        out.append(yt)
+    if withNormals is not None:
+        out.append(nt)
+    if withJacobian:
+        out.append(Jt)
+    return [output_like(x0, t) for t in out]
+
+
+def landmarkEPDiff(T, x0, a0, KparDiff, affine=None, withJacobian=False, withNormals=None, withPointSet=None):
+    """Momentum-carrying (EPDiff) shooting (pointEvolution.py:599-658); returns (xt, at)."""
+    _check_affine(affine)
+    if withJacobian or withNormals is not None or withPointSet is not None:
+        raise NotImplementedError("landmarkEPDiff optional outputs are not provided")
+    require_cuda()
+    x0d, a0d = to_dev(x0), to_dev(a0)
+    n, d = x0d.shape
+    sigma, order, sfx = _kernel_args(KparDiff)
+    xt = torch.empty((T + 1, n, d), dtype=torch.float64, device=x0d.device)
+    at = torch.zeros((T, n, d), dtype=torch.float64, device=x0d.device)
+    wsb = _lib.query("lddmm_epdiff_%s_workspace" % sfx, n, d, T)
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_epdiff_" + sfx, ptr(x0d), n, d, ptr(a0d), int(T), sigma, order, ptr(xt), ptr(at), ptr(ws), wsb,
+              stream_handle())
+    return output_like(x0, xt), output_like(x0, at)
+
+
+def landmarkHamiltonianCovector(x0, at, px1, KparDiff, regweight, affine=None):
+    """Re-shoots, then integrates the covector backwards (pointEvolution.py:735-765); returns (pxt, xt)."""
+    _check_affine(affine)
+    xt, _ = shoot(x0, at, KparDiff)
+    pxt, _ = covector(xt, at, px1, KparDiff, regweight, with_dat=False)
+    return output_like(x0, pxt), output_like(x0, xt)
+
+
+def landmarkHamiltonianGradient(x0, at, px1, KparDiff, regweight, getCovector=False, affine=None):
+    """dat_k = 2 rw a_k - p_{k+1} (pointEvolution.py:793-817).  Returns (dat, xt[, pxt]);
+    with a (zero) affine argument the reference also returns zero dA, db."""
+    _check_affine(affine)
+    xt, _ = shoot(x0, at, KparDiff)
+    pxt, dat = covector(xt, at, px1, KparDiff, regweight, with_dat=True)
+    dat_o, xt_o, pxt_o = output_like(x0, dat), output_like(x0, xt), output_like(x0, pxt)
+    if affine is None:
+        return (dat_o, xt_o, pxt_o) if getCovector else (dat_o, xt_o)
+    dA = np.zeros(np.shape(affine[0])) if not is_device(x0) else torch.zeros_like(to_dev(affine[0]))
+    db = np.zeros(np.shape(affine[1])) if not is_device(x0) else torch.zeros_like(to_dev(affine[1]))
+    return (dat_o, dA, db, xt_o, pxt_o) if getCovector else (dat_o, dA, db, xt_o)

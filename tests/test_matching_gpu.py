@@ -1,0 +1,91 @@
+"""GPU parity of the full matching problems (cg + shooting + adjoint + data
+terms) against the objective traces recorded from the reference's own
+SurfaceMatching / CurveMatching / cg (tests/golden).
+
+Tolerance: fp64 path, every accepted objective within 1e-9 relative; fp32c
+path, within 1e-6 relative (the final-energy bar), same number of iterations.
+"""
+import logging
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32c": 1e-6, "fp64": 1e-9}
+
+
+def _trace(obj):
+    trace = []
+    orig = obj.acceptVarTry
+
+    def accept():
+        orig()
+        trace.append(float(obj.obj))
+
+    obj.acceptVarTry = accept
+    return trace
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("err", ["varifold", "current", "measure"])
+def test_surface_matching_trace(golden, precision, err):
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+    f, v0, v1 = golden["sm_faces"], golden["sm_v0"], golden["sm_v1"]
+    param = SM.SurfaceMatchingParam(timeStep=0.2, KparDiff=kf.Kernel(name="gauss", sigma=0.4, precision=precision),
+                                    KparDist=kf.Kernel(name="gauss", sigma=0.3, precision=precision),
+                                    sigmaError=0.5, errorType=err)
+    sm = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v0]), Target=sf.Surface(FV=[f, v1]), param=param, maxIter=6,
+                            testGradient=False)
+    trace = _trace(sm)
+    sm.optimizeMatching()
+    ref = golden["sm_%s_trace" % err]
+    got = np.array([sm.obj0] + trace)
+    assert got.shape == ref.shape, (got, ref)
+    np.testing.assert_allclose(got, ref, rtol=TOL[precision])
+    np.testing.assert_allclose(sm.at.cpu().numpy(), golden["sm_%s_at" % err], rtol=0,
+                               atol=100 * TOL[precision] * np.abs(golden["sm_%s_at" % err]).max())
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("err", ["current", "measure"])
+def test_curve_matching_trace(golden, precision, err):
+    from registration_b200 import curveMatching as CM
+    from registration_b200 import curves as cv
+    from registration_b200 import kernelFunctions as kf
+    param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
+                                  KparDist=kf.Kernel(name="gauss", sigma=0.5, precision=precision), sigmaError=1.0,
+                                  errorType=err)
+    cm = CM.CurveMatching(Template=cv.Curve(pointSet=golden["cm_v0"]), Target=cv.Curve(pointSet=golden["cm_v1"]),
+                          param=param, maxIter=8, saveRate=0)
+    trace = _trace(cm)
+    cm.optimizeMatching()
+    ref = golden["cm_%s_trace" % err]
+    got = np.array([cm.obj0] + trace)
+    assert got.shape == ref.shape, (got, ref)
+    np.testing.assert_allclose(got, ref, rtol=TOL[precision])
+
+
+def test_user_plugged_data_term_is_honoured(golden):
+    """SurfaceMatchingParam's fun_obj triple is a plug-in point: a user triple is called."""
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+    calls = {"n": 0}
+
+    def my_def(a, b, K):
+        calls["n"] += 1
+        return sf.currentNormDef(a, b, K)
+
+    f, v0, v1 = golden["sm_faces"], golden["sm_v0"], golden["sm_v1"]
+    param = SM.SurfaceMatchingParam(timeStep=0.2, KparDiff=kf.Kernel(name="gauss", sigma=0.4),
+                                    KparDist=kf.Kernel(name="gauss", sigma=0.3), sigmaError=0.5, errorType="current")
+    param.fun_obj = my_def
+    sm = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v0]), Target=sf.Surface(FV=[f, v1]), param=param, maxIter=2,
+                            testGradient=True)
+    logging.disable(logging.INFO)
+    sm.optimizeMatching()
+    logging.disable(logging.NOTSET)
+    assert calls["n"] > 0
