@@ -7,6 +7,14 @@ Momenta, trajectory, directions and shapes stay on the GPU (FP64 storage);
 every objective value and dot product is reduced in FP64 on the device and
 read back as one host double, which is what the line search compares.
 
+Precision: kernel sums (shooting, adjoint, data-term gradient, dot products)
+follow the kernels' own precision.  The data-term VALUE that the line search
+compares is evaluated with an FP64 copy of KparDist by default
+(lineSearchPrecision='fp64'): the reference's stop test is an absolute
+|obj - objTry| < 1e-6 on objectives that are differences of norms of order
+|S|^2 (1e2 for a unit sphere at sigmaError 0.5), i.e. ~1e-9 relative, which an
+FP32 pair evaluation (~3e-7 relative error per term) cannot resolve.
+
 Two reuses that do not change any value: the trajectory of an accepted trial
 step is kept instead of re-shooting it in endOfIteration, and getGradient
 runs the adjoint on that stored trajectory instead of re-shooting inside
@@ -33,7 +41,7 @@ class Direction:
 class DeviceMatching:
     """Subclasses set: fv0, fv1 (shapes), param, norm_name, tgt_vectors_attr."""
 
-    def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric):
+    def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision='fp64'):
         require_cuda()
         if affine not in ('none', None):
             raise NotImplementedError("affine registration components are not provided (affine='none' only)")
@@ -65,6 +73,12 @@ class DeviceMatching:
         self._tv = to_dev(getattr(self.fv1, self.tgt_vectors_attr))
         self.fvDef.updateVertices(self.x0)
         self._fast_data = self._our_norm_functions()
+        K = self.param.KparDist
+        if lineSearchPrecision == K.precision:
+            self._Kval = K
+        else:
+            self._Kval = type(K)(name=K.name, sigma=K.sigma, order=K.order, weight=K.weight,
+                                 precision=lineSearchPrecision)
 
     # -- data term ------------------------------------------------------------
     def _our_norm_functions(self):
@@ -82,11 +96,11 @@ class DeviceMatching:
         """fun_obj(fvDef, fv1, KparDist) / sigmaError^2 as a device scalar."""
         if self._fast_data:
             e, _ = _dt.dataterm(self.param.errorType, vertices, self._dshape, self._tc, self._tv,
-                                self.param.KparDist, energy=True, grad=False)
+                                self._Kval, energy=True, grad=False)
             return e / (self.param.sigmaError ** 2)
         ff = self.shape_copy(self.fvDef)
         ff.updateVertices(vertices)
-        return torch.tensor(self.param.fun_obj(ff, self.fv1, self.param.KparDist) / self.param.sigmaError ** 2,
+        return torch.tensor(self.param.fun_obj(ff, self.fv1, self._Kval) / self.param.sigmaError ** 2,
                             dtype=torch.float64, device=self.x0.device)
 
     def dataTerm(self, _fvDef, _fvInit=None):
@@ -116,7 +130,7 @@ class DeviceMatching:
     def objectiveFun(self):
         """(surfaceMatching.py:233-250)"""
         if self.obj is None:
-            self.obj0 = self.param.fun_obj0(self.fv1, self.param.KparDist) / (self.param.sigmaError ** 2)
+            self.obj0 = self.param.fun_obj0(self.fv1, self._Kval) / (self.param.sigmaError ** 2)
             xt, e = evol.shoot(self.x0, self.at, self.param.KparDiff, regweight=self.regweight, with_energy=True)
             self.xt = xt
             self.fvDef.updateVertices(xt[-1])

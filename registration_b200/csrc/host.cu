@@ -63,13 +63,15 @@ int check_device_ptr(const void* ptr, const char* name) {
     return LDDMM_OK;
 }
 
-void laplacian_tables(int order, double P[5], double Q[4], double Rr[3]) {
+void laplacian_tables(int order, double P[5], double Q[4], double Rr[3], bool exact) {
     // rows of c_, c1_, c2_ (kernelFunctions.f90:24-26, 85-86, 325); the
-    // literals are default-real, i.e. float32-rounded.
-    const double t3 = (double)(1.0f / 3.0f), t04 = (double)0.4f, t37 = (double)(3.0f / 7.0f);
-    const double t15 = (double)(1.0f / 15.0f), t221 = (double)(2.0f / 21.0f), t105 = (double)(1.0f / 105.0f);
-    const double t5 = (double)(1.0f / 5.0f), t7 = (double)(1.0f / 7.0f), t235 = (double)(2.0f / 35.0f);
-    const double t35 = (double)(1.0f / 35.0f);
+    // literals are default-real, i.e. float32-rounded, unless `exact`.
+    const double t3 = exact ? 1.0 / 3 : (double)(1.0f / 3.0f), t04 = exact ? 0.4 : (double)0.4f;
+    const double t37 = exact ? 3.0 / 7 : (double)(3.0f / 7.0f);
+    const double t15 = exact ? 1.0 / 15 : (double)(1.0f / 15.0f), t221 = exact ? 2.0 / 21 : (double)(2.0f / 21.0f);
+    const double t105 = exact ? 1.0 / 105 : (double)(1.0f / 105.0f);
+    const double t5 = exact ? 1.0 / 5 : (double)(1.0f / 5.0f), t7 = exact ? 1.0 / 7 : (double)(1.0f / 7.0f);
+    const double t235 = exact ? 2.0 / 35 : (double)(2.0f / 35.0f), t35 = exact ? 1.0 / 35 : (double)(1.0f / 35.0f);
     const double p[5][5] = {{1, 0, 0, 0, 0}, {1, 1, 0, 0, 0}, {1, 1, t3, 0, 0}, {1, 1, t04, t15, 0},
                             {1, 1, t37, t221, t105}};
     const double q[5][4] = {{0, 0, 0, 0}, {1, 0, 0, 0}, {t3, t3, 0, 0}, {t5, t5, t15, 0}, {t7, t7, t235, t105}};

@@ -72,7 +72,9 @@ inline int cuda_check(cudaError_t e, const char* what) {
     } while (0)
 
 // Laplacian polynomial tables of py-lddmm/kernelFunctions.f90 (c_ :24-26,
-// c1_ :85-86, c2_ :325) with their default-real (float32) literal values.
-void laplacian_tables(int order, double P[5], double Q[4], double Rr[3]);
+// c1_ :85-86, c2_ :325) with their default-real (float32) literal values, or
+// (exact = true) the exact rationals of the dense numpy path lapPol /
+// lapPolDiff / lapPolDiff2 (kernelFunctions.py:58-103).
+void laplacian_tables(int order, double P[5], double Q[4], double Rr[3], bool exact = false);
 
 }  // namespace lddmm

@@ -288,7 +288,9 @@ int div_impl(const ApplyKArgs& a, Workspace& ws, cudaStream_t st) {
     double* part = ws.take<double>((size_t)pl.split * a.n);
     double* center = ws.take<double>(4);
     if (ws.measuring()) return LDDMM_OK;
-    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
+    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma, /*exact_tables=*/true);
+    // (the reference's applyDivergence runs on its dense numpy matrices, which
+    //  use the exact rational polynomials, kernelFunctions.py:75-88)
     typename Op::Params P{};
     P.src4 = src;
     P.src_stride = pl.m_pad;

@@ -35,12 +35,37 @@ static __global__ void probe_ex2_kernel(float* out, int iters) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// 8 independent packed-pair FMA chains (fma.rn.f32x2, sm_100a): 8*iters
+// instructions, 16*iters FMAs per thread.
+static __global__ void probe_ffma2_kernel(float* out, int iters) {
+    unsigned long long x[8], a, b;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(0.999f), "f"(0.998f));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(1e-4f), "f"(2e-4f));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const float u = (threadIdx.x + j) * 1e-3f;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(x[j]) : "f"(u), "f"(u + 0.5f));
+    }
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) asm("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(x[j]) : "l"(a), "l"(b));
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        float p, q;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(p), "=f"(q) : "l"(x[j]));
+        s += p + q;
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace lddmm
 
 extern "C" LDDMM_API int lddmm_probe_launch(int what, int blocks, int threads, int iters, float* out,
                                             lddmm_stream_t stream) {
     using namespace lddmm;
-    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || (what != 0 && what != 1)) {
+    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || what < 0 || what > 2) {
         set_error("probe: invalid launch (what=%d blocks=%d threads=%d iters=%d)", what, blocks, threads, iters);
         return LDDMM_ERR_ARG;
     }
@@ -48,7 +73,9 @@ extern "C" LDDMM_API int lddmm_probe_launch(int what, int blocks, int threads, i
     cudaStream_t st = (cudaStream_t)stream;
     if (what == 0)
         probe_ffma_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999f, 1e-4f);
-    else
+    else if (what == 1)
         probe_ex2_kernel<<<blocks, threads, 0, st>>>(out, iters);
+    else
+        probe_ffma2_kernel<<<blocks, threads, 0, st>>>(out, iters);
     return cuda_check(cudaGetLastError(), "probe launch");
 }

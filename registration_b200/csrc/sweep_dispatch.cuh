@@ -60,10 +60,10 @@ struct KScale {
 };
 
 template <class Real>
-KScale kernel_scale(int kind, int order, double sigma) {
+KScale kernel_scale(int kind, int order, double sigma, bool exact_tables = false) {
     KScale k{};
     double P[5], Q[4], Rr[3];
-    laplacian_tables(order, P, Q, Rr);
+    laplacian_tables(order, P, Q, Rr, exact_tables);
     const double L = 1.4426950408889634;  // log2(e)
     if (sizeof(Real) == 4) {
         k.scale = (kind == KGAUSS) ? std::sqrt(0.5 * L) / sigma : L / sigma;

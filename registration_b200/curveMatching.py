@@ -52,7 +52,7 @@ class CurveMatching(DeviceMatching):
         self.saveRate = saveRate
         self.saveFile = saveFile
         self.outputDir = outputDir
-        self._init_state(maxIter, regWeight, verb, testGradient, affine, False)
+        self._init_state(maxIter, regWeight, verb, testGradient, affine, False, lineSearchPrecision)
 
     @staticmethod
     def shape_copy(c):

@@ -9,6 +9,8 @@ errorType selects the (fun_obj0, fun_obj, fun_objGrad) plug-in triple among
 this library's surfaces.current/measure/varifold norms; a user-set triple is
 honoured too (called with Surface objects).  Only affine='none' and
 symmetric=False are provided.  VTK output of the iterates is not written.
+Extra keyword: lineSearchPrecision ('fp64' default) -- the precision of the
+data-term values compared by the line search (see registration_b200._matching).
 """
 import logging
 
@@ -46,7 +48,7 @@ class SurfaceMatching(DeviceMatching):
     def __init__(self, Template=None, Target=None, fileTempl=None, fileTarg=None, param=None, maxIter=1000,
                  regWeight=1.0, affineWeight=1.0, verb=True, subsampleTargetSize=-1, rotWeight=None,
                  scaleWeight=None, transWeight=None, symmetric=False, testGradient=True, saveFile='evolution',
-                 affine='none', outputDir='.'):
+                 affine='none', outputDir='.', lineSearchPrecision='fp64'):
         if Template is None or Target is None:
             raise ValueError('Please provide template and target surfaces (file readers are not provided)')
         if subsampleTargetSize > 0:
@@ -62,7 +64,7 @@ class SurfaceMatching(DeviceMatching):
             self.fv1.flipFaces()
         self.fvInit = surfaces.Surface(surf=self.fv0)
         self.fvDef = surfaces.Surface(surf=self.fvInit)
-        self._init_state(maxIter, regWeight, verb, testGradient, affine, symmetric)
+        self._init_state(maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision)
         self.coeffAff1 = 1.
         self.coeffAff2 = 100.
         self.coeffAff = self.coeffAff1

@@ -1,8 +1,11 @@
 """GPU parity of the surface / curve data-attachment norms and gradients.
 
 Against the reference fixtures (tests/golden) and the FP64 oracle.
-Tolerance: fp32c 1e-5 relative (values: |e - e_ref| / max(|e_ref|, |norm0|);
-gradients: max-abs difference / max-abs reference), fp64 1e-11.
+Tolerance: fp32c 1e-5, fp64 1e-11, relative to the magnitude of the summed
+terms: values against |Norm0| of the target; gradients against the largest
+entry of the gradient of |S1|^2 alone (the target term has the same size).
+A gradient of |S1 - S2|^2 between nearby shapes is a small difference of two
+such sums, so its own magnitude is not the scale of the FP32 rounding.
 """
 import numpy as np
 import pytest
@@ -15,6 +18,13 @@ TOL = {"fp32c": 1e-5, "fp64": 1e-11}
 def rel(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def self_scale(ref_mod, shape_cls, fvD, grad_fn, K, vec_attr, **kw):
+    """max |gradient of |S1|^2| computed by the oracle against a null target."""
+    tgt = shape_cls(**kw)
+    setattr(tgt, vec_attr, np.zeros_like(getattr(tgt, vec_attr)))
+    return np.abs(grad_fn(fvD, tgt, K)).max()
 
 
 @pytest.fixture(scope="module")
@@ -41,7 +51,11 @@ def test_surface_norms_golden(golden, mods, precision, kname, sig, err):
     nd = getattr(sf, err + "NormDef")(fvD, fv1, K)
     assert abs(nd - golden[p + "normdef"]) <= TOL[precision] * max(scale, abs(float(golden[p + "normdef"])))
     g = getattr(sf, err + "NormGradient")(fvD, fv1, K)
-    assert rel(g, golden[p + "grad"]) < TOL[precision]
+    from oracle import lddmm_ref as ref
+    KR = ref.Kernel(name=kname, sigma=sig)
+    G = self_scale(ref, ref.Surface, ref.Surface(FV=[f, golden["surf_vdef"]]), getattr(ref, err + "NormGradient"),
+                   KR, "surfel", FV=[f, golden["surf_vtgt"]])
+    assert np.abs(g - golden[p + "grad"]).max() < TOL[precision] * max(G, np.abs(golden[p + "grad"]).max())
 
 
 @pytest.mark.parametrize("precision", ["fp32c", "fp64"])
@@ -56,7 +70,12 @@ def test_curve_norms_golden(golden, mods, precision, kname, err):
     scale = abs(float(golden[p + "norm0"]))
     assert abs(getattr(cv, err + "Norm0")(fv1, K) - golden[p + "norm0"]) <= TOL[precision] * scale
     assert abs(getattr(cv, err + "NormDef")(fvD, fv1, K) - golden[p + "normdef"]) <= TOL[precision] * scale
-    assert rel(getattr(cv, err + "NormGradient")(fvD, fv1, K), golden[p + "grad"]) < TOL[precision]
+    from oracle import lddmm_ref as ref
+    KR = ref.Kernel(name=kname, sigma=0.5)
+    G = self_scale(ref, ref.Curve, ref.Curve(pointSet=golden["curve_vdef"]), getattr(ref, "curve_" + err +
+                   "NormGradient"), KR, "lenel", pointSet=golden["curve_vtgt"])
+    g = getattr(cv, err + "NormGradient")(fvD, fv1, K)
+    assert np.abs(g - golden[p + "grad"]).max() < TOL[precision] * max(G, np.abs(golden[p + "grad"]).max())
 
 
 @pytest.mark.parametrize("precision", ["fp32c", "fp64"])
