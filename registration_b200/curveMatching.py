@@ -41,7 +41,7 @@ class CurveMatching(DeviceMatching):
     def __init__(self, Template=None, Target=None, fileTempl=None, fileTarg=None, param=None, maxIter=1000,
                  regWeight=1.0, affineWeight=1.0, verb=True, gradLB=0.001, saveRate=10, rotWeight=None,
                  scaleWeight=None, transWeight=None, testGradient=False, saveFile='evolution', affine='none',
-                 outputDir='.'):
+                 outputDir='.', lineSearchPrecision='fp64'):
         if Template is None or Target is None:
             raise ValueError('Please provide template and target curves (file readers are not provided)')
         self.fv0 = curves.Curve(curve=Template)
