@@ -67,6 +67,19 @@ LDDMM_API size_t lddmm_applyk_f32c_workspace(int64_t n, int64_t m, int d, int di
 LDDMM_API int lddmm_applyk_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d, int dimb,
                       double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
                       lddmm_stream_t stream);
+/* Allocation-free variant of lddmm_applyk_f32c -- no counterpart in the
+ * reference.  For callers that cannot allocate GPU memory (a plug-in whose
+ * host framework owns all device allocations, an FFI caller without a CUDA
+ * allocator, a path where cudaMalloc / cudaFree would synchronise the device):
+ * the caller passes the inputs and the output only, and the scratch memory is a
+ * 32 MiB array in the library's static device memory (held by every GPU that
+ * loads the library until exit).  Shapes whose scratch exceeds 32 MiB (about
+ * n = m = 400,000 with dimb <= 4) return LDDMM_ERR_WORKSPACE before any launch.
+ * All calls on a device share that array: calls that overlap on the GPU race,
+ * so order them on one stream.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress); make it before any stream capture. */
+LDDMM_API int lddmm_applyk_f32c_noalloc(const double* x, int64_t n, const double* y, int64_t m, const double* beta,
+                                        int d, int dimb, double sigma, int order, double* f, lddmm_stream_t stream);
 LDDMM_API size_t lddmm_applyk_f64_workspace(int64_t n, int64_t m, int d, int dimb);
 LDDMM_API int lddmm_applyk_f64(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d, int dimb,
                      double sigma, int order, double* f, void* workspace, size_t workspace_bytes,

@@ -3,6 +3,7 @@
 #include <type_traits>
 
 #include "host.h"
+#include "internal.h"
 #include "pack.cuh"
 #include "sweep_dispatch.cuh"
 
@@ -21,12 +22,13 @@ struct ApplyKArgs {
     double sigma;
     int order;
     double* f;
+    int split_cap;  // 0: no cap on the number of source chunks
 };
 
 template <class Real, int KIND, int DEG, int D, int DIMB>
 int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) {
     using Op = OpApplyK<Real, KIND, DEG, D, DIMB>;
-    const SinglePlan pl = plan_single<Op>(a.n, a.m);
+    const SinglePlan pl = plan_single<Op>(a.n, a.m, a.split_cap);
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * DIMB);
@@ -113,7 +115,7 @@ static int applyk_validate(const ApplyKArgs& a) {
 
 template <class Real>
 size_t applyk_ws(int64_t n, int64_t m, int d, int dimb) {
-    ApplyKArgs a{nullptr, n, nullptr, m, nullptr, d, dimb, 1.0, 10, nullptr};
+    ApplyKArgs a{nullptr, n, nullptr, m, nullptr, d, dimb, 1.0, 10, nullptr, 0};
     if (n <= 0 || m <= 0 || d < 1 || d > 3 || dimb < 1) return 0;
     Workspace ws;
     applyk_run<Real>(a, ws, 0);
@@ -327,7 +329,7 @@ int div_run(const ApplyKArgs& a, Workspace& ws, cudaStream_t st) {
 template <class Real>
 size_t div_ws(int64_t n, int64_t m, int d) {
     if (n <= 0 || m <= 0 || d < 1 || d > 3) return 0;
-    ApplyKArgs a{nullptr, n, nullptr, m, nullptr, d, d, 1.0, 10, nullptr};
+    ApplyKArgs a{nullptr, n, nullptr, m, nullptr, d, d, 1.0, 10, nullptr, 0};
     Workspace ws;
     div_run<Real>(a, ws, 0);
     return ws.off + 256;
@@ -355,6 +357,26 @@ int div_entry(const ApplyKArgs& a, void* wsp, size_t wsb, cudaStream_t st) {
     return div_run<Real>(a, ws, st);
 }
 
+size_t applyk_f32c_scratch_bytes(int64_t n, int64_t m, int d, int dimb, int split_cap) {
+    if (n <= 0 || m <= 0 || d < 1 || d > 3 || dimb < 1) return 0;
+    ApplyKArgs a{nullptr, n, nullptr, m, nullptr, d, dimb, 1.0, 10, nullptr, split_cap};
+    size_t best = 0;
+    for (int order : {10, 3}) {  // Gaussian and Laplacian plans
+        a.order = order;
+        Workspace ws;
+        applyk_run<float>(a, ws, 0);
+        best = std::max(best, ws.off);
+    }
+    return best + 256;
+}
+
+int applyk_f32c_in_workspace(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d,
+                             int dimb, double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                             cudaStream_t stream, int split_cap) {
+    ApplyKArgs a{x, n, y, m, beta, d, dimb, sigma, order, f, split_cap};
+    return applyk_entry<float>(a, workspace, workspace_bytes, stream);
+}
+
 }  // namespace lddmm
 
 using namespace lddmm;
@@ -367,14 +389,14 @@ size_t lddmm_applyk_f64_workspace(int64_t n, int64_t m, int d, int dimb) { retur
 int lddmm_applyk_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d, int dimb,
                       double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
                       lddmm_stream_t stream) {
-    ApplyKArgs a{x, n, y, m, beta, d, dimb, sigma, order, f};
+    ApplyKArgs a{x, n, y, m, beta, d, dimb, sigma, order, f, 0};
     return applyk_entry<float>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 int lddmm_applyk_f64(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d, int dimb,
                      double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
                      lddmm_stream_t stream) {
-    ApplyKArgs a{x, n, y, m, beta, d, dimb, sigma, order, f};
+    ApplyKArgs a{x, n, y, m, beta, d, dimb, sigma, order, f, 0};
     return applyk_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
@@ -404,13 +426,13 @@ size_t lddmm_applydiv_f64_workspace(int64_t n, int64_t m, int d) { return div_ws
 
 int lddmm_applydiv_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* a, int d, double sigma,
                         int order, double* f, void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
-    ApplyKArgs q{x, n, y, m, a, d, d, sigma, order, f};
+    ApplyKArgs q{x, n, y, m, a, d, d, sigma, order, f, 0};
     return div_entry<float>(q, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 int lddmm_applydiv_f64(const double* x, int64_t n, const double* y, int64_t m, const double* a, int d, double sigma,
                        int order, double* f, void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
-    ApplyKArgs q{x, n, y, m, a, d, d, sigma, order, f};
+    ApplyKArgs q{x, n, y, m, a, d, d, sigma, order, f, 0};
     return div_entry<double>(q, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

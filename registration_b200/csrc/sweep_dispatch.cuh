@@ -25,7 +25,7 @@ struct SinglePlan {
 };
 
 template <class Op>
-SinglePlan plan_single(long long n, long long m) {
+SinglePlan plan_single(long long n, long long m, int split_cap = 0) {
     SinglePlan p;
     const long long per_block = (long long)Op::BLOCK * Op::R;
     p.n_tb = (int)((n + per_block - 1) / per_block);
@@ -33,6 +33,7 @@ SinglePlan plan_single(long long n, long long m) {
     p.n_src_tiles = (int)((m + Op::TILE - 1) / Op::TILE);
     p.m_pad = (long long)std::max(p.n_src_tiles, 1) * Op::TILE;
     p.split = choose_split(p.n_tb, p.n_src_tiles, sweep_slots<Op>());
+    if (split_cap > 0 && p.split > split_cap) p.split = split_cap;
     return p;
 }
 
