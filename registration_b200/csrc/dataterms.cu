@@ -66,6 +66,7 @@ struct OpData {
     using Real = Real_;
     using L = DataLayout<MODE, D>;
     static constexpr bool F32 = sizeof(Real) == 4;
+    static constexpr int TPS = 1;
     static constexpr int BLOCK = 128, R = 2, TILE = 128, FOLD = F32 ? 32 : TILE;
     static constexpr int PP = PointPlanes<Real>::N;
     static constexpr int PW = Traits<Real>::PER_WORD;

@@ -4,6 +4,7 @@
 
 #include "host.h"
 #include "internal.h"
+#include "ops2.cuh"
 #include "pack.cuh"
 #include "sweep_dispatch.cuh"
 
@@ -27,7 +28,9 @@ struct ApplyKArgs {
 
 template <class Real, int KIND, int DEG, int D, int DIMB>
 int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) {
-    using Op = OpApplyK<Real, KIND, DEG, D, DIMB>;
+    // FP32: packed-pair operator (two targets per slot, duplicated source records);
+    // FP64: the plain operator on double records.
+    using Op = std::conditional_t<sizeof(Real) == 4, OpApplyK2<KIND, DEG, D, DIMB>, OpApplyK<Real, KIND, DEG, D, DIMB>>;
     const SinglePlan pl = plan_single<Op>(a.n, a.m, a.split_cap);
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
@@ -44,20 +47,27 @@ int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) 
     P.src_stride = pl.m_pad;
     P.tgt4 = tgt;
     P.tgt_stride = pl.n_tpad;
-    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
-    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
-    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
-                                                                  pl.n_tpad);
-    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
-                                                                 pl.m_pad);
     Gather g{};
     g.src = a.beta;
     g.row_stride = a.dimb;
     g.nvals = std::min(DIMB, a.dimb - col0);
     for (int c = 0; c < g.nvals; ++c) g.off[c] = col0 + c;
     g.mult = 1.0;
-    pack_values_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(g, a.m, src, pl.m_pad, pl.m_pad, Op::PP);
+    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
+                                                                  pl.n_tpad);
+    if constexpr (sizeof(Real) == 4) {
+        for (int j = 0; j < 5; ++j) P.pkd[j] = dup_coeff(ks.pk[j]);
+        for (int j = 0; j < 4; ++j) P.pqd[j] = dup_coeff(ks.pq[j]);
+        pack_dup_kernel<<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, g, D, DIMB, src,
+                                                            pl.m_pad, pl.m_pad);
+    } else {
+        for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
+        for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+        pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
+                                                                     pl.m_pad);
+        pack_values_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(g, a.m, src, pl.m_pad, pl.m_pad, Op::PP);
+    }
     LDDMM_TRY(launch_single<Op>(pl, a.n, P, part, st));
     // combine writes only the group's own columns
     const int ncols = g.nvals;
@@ -164,9 +174,10 @@ struct DiffKTArgs {
 
 template <class Real, int KIND, int DEG, int D, int W>
 int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
-    using Op = OpDiffKT<Real, KIND, DEG, D, W>;
+    using Op = std::conditional_t<sizeof(Real) == 4, OpDiffKT2<KIND, DEG, D, W>, OpDiffKT<Real, KIND, DEG, D, W>>;
+    constexpr int NT = (sizeof(Real) == 4) ? 1 + (W + 3) / 4 : Op::NS;  // target planes
     const SinglePlan pl = plan_single<Op>(a.n, a.m);
-    float4* tgt = ws.take<float4>((size_t)Op::NS * pl.n_tpad);
+    float4* tgt = ws.take<float4>((size_t)NT * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * D);
     double* center = ws.take<double>(4);
@@ -177,13 +188,6 @@ int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
     P.src_stride = pl.m_pad;
     P.tgt4 = tgt;
     P.tgt_stride = pl.n_tpad;
-    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
-    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
-    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
-                                                                  pl.n_tpad);
-    pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
-                                                                 pl.m_pad);
     // u_k / v_l: value w = c*na + i  <->  a[i, row, c]  (the Fortran sum order)
     Gather gu{}, gv{};
     gu.src = a.a1;
@@ -196,8 +200,23 @@ int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
         gu.off[w] = (long long)i * a.n * a.dimb + c;
         gv.off[w] = (long long)i * a.m * a.dimb + c;
     }
-    pack_values_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(gu, a.n, tgt, pl.n_tpad, pl.n_tpad, Op::PP);
-    pack_values_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(gv, a.m, src, pl.m_pad, pl.m_pad, Op::PP);
+    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
+                                                                  pl.n_tpad);
+    pack_values_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(gu, a.n, tgt, pl.n_tpad, pl.n_tpad,
+                                                                  PointPlanes<Real>::N);
+    if constexpr (sizeof(Real) == 4) {
+        for (int j = 0; j < 5; ++j) P.pkd[j] = dup_coeff(ks.pk[j]);
+        for (int j = 0; j < 4; ++j) P.pqd[j] = dup_coeff(ks.pq[j]);
+        pack_dup_kernel<<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, gv, D, W, src,
+                                                            pl.m_pad, pl.m_pad);
+    } else {
+        for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
+        for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+        pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,
+                                                                     pl.m_pad);
+        pack_values_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(gv, a.m, src, pl.m_pad, pl.m_pad, Op::PP);
+    }
     LDDMM_TRY(launch_single<Op>(pl, a.n, P, part, st));
     const int dout = a.d;  // D may exceed d (d == 1 runs as D == 2)
     if (dout == D) {

@@ -113,6 +113,7 @@ template <class Real_, int KIND, int DEG, int D, int DIMB>
 struct OpApplyK {
     using Real = Real_;
     static constexpr bool F32 = sizeof(Real) == 4;
+    static constexpr int TPS = 1;
     static constexpr int BLOCK = 128;
     static constexpr int R = F32 ? 4 : 2;
     static constexpr int TILE = 128;
@@ -157,6 +158,7 @@ template <class Real_, int KIND, int DEG, int D, int W>
 struct OpDiffKT {
     using Real = Real_;
     static constexpr bool F32 = sizeof(Real) == 4;
+    static constexpr int TPS = 1;
     static constexpr int BLOCK = 128;
     static constexpr int R = 2;
     static constexpr int TILE = 128;
@@ -208,6 +210,7 @@ template <class Real_, int KIND, int DEG, int D>
 struct OpDivergence {
     using Real = Real_;
     static constexpr bool F32 = sizeof(Real) == 4;
+    static constexpr int TPS = 1;
     static constexpr int BLOCK = 128;
     static constexpr int R = 4;
     static constexpr int TILE = 128;

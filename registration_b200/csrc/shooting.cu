@@ -20,6 +20,7 @@
 // step's energy partials (one per combine block; the grid size depends only on
 // n, so the reduction order is fixed).
 #include "host.h"
+#include "ops2.cuh"
 #include "pack.cuh"
 #include "sweep_dispatch.cuh"
 
@@ -63,6 +64,21 @@ LDDMM_D void zero_record(float4* planes, long long stride, long long i, int npla
     for (int p = 0; p < nplanes; ++p) planes[(long long)p * stride + i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// Duplicated source record (packed-pair FP32 operators, ops2.cuh): values
+// [(x - c) * s for D coordinates, vals[0..nv) padded to V], each value twice.
+LDDMM_D void store_dup(float4* planes, long long stride, long long i, const double* x, int d, int D, double s,
+                       const double* c, const double* vals, int nv, int V) {
+    float v[16];
+    const int NV = D + V;
+    for (int q = 0; q < NV; ++q) v[q] = 0.f;
+    for (int j = 0; j < d; ++j) v[j] = (float)((x[j] - c[j]) * s);
+    for (int q = 0; q < nv && q < V; ++q) v[D + q] = (float)vals[q];
+    for (int w = 0; w < (NV + 1) / 2; ++w) {
+        const float a = v[2 * w], b = (2 * w + 1 < NV) ? v[2 * w + 1] : 0.f;
+        planes[(long long)w * stride + i] = make_float4(a, a, b, b);
+    }
+}
+
 // block-level FP64 sum with a fixed tree; thread 0 writes out[blockIdx.x]
 LDDMM_D void block_sum_store(double v, double* out) {
     __shared__ double red[kCombineThreads];
@@ -75,9 +91,23 @@ LDDMM_D void block_sum_store(double v, double* out) {
     if (threadIdx.x == 0) out[blockIdx.x] = red[0];
 }
 
+// kernel polynomials into either parameter block
+inline void set_poly(KernelParamsBase<double>& P, const KScale& ks) {
+    for (int j = 0; j < 5; ++j) P.pk[j] = ks.pk[j];
+    for (int j = 0; j < 4; ++j) P.pq[j] = ks.pq[j];
+}
+inline void set_poly(KernelParamsBase<float>& P, const KScale& ks) {
+    for (int j = 0; j < 5; ++j) P.pk[j] = (float)ks.pk[j];
+    for (int j = 0; j < 4; ++j) P.pq[j] = (float)ks.pq[j];
+}
+inline void set_poly(KernelParams2& P, const KScale& ks) {
+    for (int j = 0; j < 5; ++j) P.pkd[j] = dup_coeff(ks.pk[j]);
+    for (int j = 0; j < 4; ++j) P.pqd[j] = dup_coeff(ks.pq[j]);
+}
+
 // ---- shooting ---------------------------------------------------------------
 // Packs step-0 planes: targets (pos) and sources (pos, a).
-template <class Real>
+template <class Real, bool DUP>
 static __global__ void shoot_pack_kernel(const double* __restrict__ x, const double* __restrict__ a, long long n,
                                          int d, double s, const double* __restrict__ c, float4* tgt,
                                          long long tstride, float4* src, long long sstride, int pp, int nslots,
@@ -88,8 +118,12 @@ static __global__ void shoot_pack_kernel(const double* __restrict__ x, const dou
         if (i < n) {
             if (i < tstride) store_point<Real>(tgt, tstride, i, x + i * d, d, s, c);
             if (i < sstride) {
-                store_point<Real>(src, sstride, i, x + i * d, d, s, c);
-                store_vals<Real>(src, sstride, i, pp, a + i * d, d, nslots);
+                if constexpr (DUP) {
+                    store_dup(src, sstride, i, x + i * d, d, nslots, s, c, a + i * d, d, nslots);
+                } else {
+                    store_point<Real>(src, sstride, i, x + i * d, d, s, c);
+                    store_vals<Real>(src, sstride, i, pp, a + i * d, d, nslots);
+                }
             }
         } else {
             if (i < tstride) zero_record<Real>(tgt, tstride, i, pp);
@@ -99,7 +133,7 @@ static __global__ void shoot_pack_kernel(const double* __restrict__ x, const dou
 }
 
 // v = sum of chunks; x1 = x0 + dt v; energy partial <a, v>; pack next step.
-template <class Real>
+template <class Real, bool DUP>
 static __global__ void shoot_combine_kernel(const double* __restrict__ part, long long n, int d, int dout,
                                             int split, double dt, const double* __restrict__ x0,
                                             const double* __restrict__ a0, double* __restrict__ x1,
@@ -119,8 +153,12 @@ static __global__ void shoot_combine_kernel(const double* __restrict__ part, lon
         }
         if (a1 != nullptr) {
             store_point<Real>(tgt, tstride, i, xn, d, s, c);
-            store_point<Real>(src, sstride, i, xn, d, s, c);
-            store_vals<Real>(src, sstride, i, pp, a1 + i * d, d, nslots);
+            if constexpr (DUP) {
+                store_dup(src, sstride, i, xn, d, nslots, s, c, a1 + i * d, d, nslots);
+            } else {
+                store_point<Real>(src, sstride, i, xn, d, s, c);
+                store_vals<Real>(src, sstride, i, pp, a1 + i * d, d, nslots);
+            }
         }
     }
     block_sum_store(e, epart);
@@ -150,7 +188,8 @@ struct ShootArgs {
 
 template <class Real, int KIND, int DEG, int D>
 int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
-    using Op = OpApplyK<Real, KIND, DEG, D, D>;
+    constexpr bool DUP = sizeof(Real) == 4;  // FP32: packed-pair operator with duplicated sources
+    using Op = std::conditional_t<DUP, OpApplyK2<KIND, DEG, D, D>, OpApplyK<Real, KIND, DEG, D, D>>;
     const SinglePlan pl = plan_single<Op>(a.n, a.n);
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
@@ -165,17 +204,16 @@ int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     P.src_stride = pl.m_pad;
     P.tgt4 = tgt;
     P.tgt_stride = pl.n_tpad;
-    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
-    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+    set_poly(P, ks);
     const long long N = a.n * a.d;
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.xt, a.x0, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "shoot copy"));
     bbox_center_kernel<<<1, 256, 0, st>>>(a.x0, a.n, nullptr, 0, a.d, center);
-    shoot_pack_kernel<Real><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
+    shoot_pack_kernel<Real, DUP><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.x0, a.at, a.n, a.d, ks.scale, center, tgt, pl.n_tpad, src, pl.m_pad, Op::PP, D, Op::NS);
     const double dt = 1.0 / a.T;
     for (int t = 0; t < a.T; ++t) {
         LDDMM_TRY(launch_single<Op>(pl, a.n, P, part, st));
-        shoot_combine_kernel<Real><<<nb, kCombineThreads, 0, st>>>(
+        shoot_combine_kernel<Real, DUP><<<nb, kCombineThreads, 0, st>>>(
             part, a.n, a.d, D, pl.split, dt, a.xt + t * N, a.at + t * N, a.xt + (t + 1) * N,
             t + 1 < a.T ? a.at + (t + 1) * N : nullptr, ks.scale, center, tgt, pl.n_tpad, src, pl.m_pad, Op::PP,
             D, epart + (long long)t * nb);
@@ -196,7 +234,7 @@ int shoot_run(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
 
 // ---- covector ---------------------------------------------------------------
 // planes of step t: targets (pos, u = (p - 2 rw a, a)), sources (pos, v = (a, p))
-template <class Real>
+template <class Real, bool DUP>
 LDDMM_D void cov_store(float4* tgt, long long tstride, float4* src, long long sstride, long long i, int pp,
                        const double* x, const double* a, const double* p, int d, double s, const double* c,
                        double rw, int tw) {
@@ -212,30 +250,34 @@ LDDMM_D void cov_store(float4* tgt, long long tstride, float4* src, long long ss
         store_vals<Real>(tgt, tstride, i, pp, u, 2 * d, tw);
     }
     if (i < sstride) {
-        store_point<Real>(src, sstride, i, x, d, s, c);
-        store_vals<Real>(src, sstride, i, pp, v, 2 * d, tw);
+        if constexpr (DUP) {
+            store_dup(src, sstride, i, x, d, tw / 2, s, c, v, 2 * d, tw);
+        } else {
+            store_point<Real>(src, sstride, i, x, d, s, c);
+            store_vals<Real>(src, sstride, i, pp, v, 2 * d, tw);
+        }
     }
 }
 
-template <class Real>
+template <class Real, bool DUP>
 static __global__ void cov_pack_kernel(const double* __restrict__ x, const double* __restrict__ a,
                                        const double* __restrict__ p, long long n, int d, double s,
                                        const double* __restrict__ c, double rw, float4* tgt, long long tstride,
-                                       float4* src, long long sstride, int pp, int nplanes, int tw) {
+                                       float4* src, long long sstride, int pp, int tplanes, int nplanes, int tw) {
     const long long npad = tstride > sstride ? tstride : sstride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npad;
          i += (long long)gridDim.x * blockDim.x) {
         if (i < n) {
-            cov_store<Real>(tgt, tstride, src, sstride, i, pp, x + i * d, a + i * d, p + i * d, d, s, c, rw, tw);
+            cov_store<Real, DUP>(tgt, tstride, src, sstride, i, pp, x + i * d, a + i * d, p + i * d, d, s, c, rw, tw);
         } else {
-            if (i < tstride) zero_record<Real>(tgt, tstride, i, nplanes);
+            if (i < tstride) zero_record<Real>(tgt, tstride, i, tplanes);
             if (i < sstride) zero_record<Real>(src, sstride, i, nplanes);
         }
     }
 }
 
 // p_t = p_{t+1} + dt * dscale * sum(chunks); dat_t = 2 rw a_t - p_{t+1}; pack step t-1.
-template <class Real>
+template <class Real, bool DUP>
 static __global__ void cov_combine_kernel(const double* __restrict__ part, long long n, int d, int dout, int split,
                                           double dt, double dscale, double rw, const double* __restrict__ p_next,
                                           const double* __restrict__ a_t, double* __restrict__ p_t,
@@ -255,7 +297,8 @@ static __global__ void cov_combine_kernel(const double* __restrict__ part, long 
             if (dat_t != nullptr) dat_t[i * d + j] = 2.0 * rw * a_t[i * d + j] - pj;
         }
         if (x_prev != nullptr)
-            cov_store<Real>(tgt, tstride, src, sstride, i, pp, x_prev + i * d, a_prev + i * d, pn, d, s, c, rw, tw);
+            cov_store<Real, DUP>(tgt, tstride, src, sstride, i, pp, x_prev + i * d, a_prev + i * d, pn, d, s, c, rw,
+                                 tw);
     }
 }
 
@@ -276,9 +319,11 @@ struct CovArgs {
 template <class Real, int KIND, int DEG, int D>
 int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr int W = 2 * D;
-    using Op = OpDiffKT<Real, KIND, DEG, D, W>;
+    constexpr bool DUP = sizeof(Real) == 4;  // FP32: packed-pair operator with duplicated sources
+    using Op = std::conditional_t<DUP, OpDiffKT2<KIND, DEG, D, W>, OpDiffKT<Real, KIND, DEG, D, W>>;
+    constexpr int NT = DUP ? 1 + (W + 3) / 4 : Op::NS;  // target planes (standard layout)
     const SinglePlan pl = plan_single<Op>(a.n, a.n);
-    float4* tgt = ws.take<float4>((size_t)Op::NS * pl.n_tpad);
+    float4* tgt = ws.take<float4>((size_t)NT * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * D);
     double* center = ws.take<double>(4);
@@ -289,21 +334,20 @@ int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     P.src_stride = pl.m_pad;
     P.tgt4 = tgt;
     P.tgt_stride = pl.n_tpad;
-    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
-    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+    set_poly(P, ks);
     const long long N = a.n * a.d;
     const double dt = 1.0 / a.T;
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.pxt + (long long)a.T * N, a.px1, sizeof(double) * N,
                                          cudaMemcpyDeviceToDevice, st), "covector copy"));
     const int T = a.T;
     bbox_center_kernel<<<1, 256, 0, st>>>(a.xt, a.n, nullptr, 0, a.d, center);
-    cov_pack_kernel<Real><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
+    cov_pack_kernel<Real, DUP><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.xt + (long long)(T - 1) * N, a.at + (long long)(T - 1) * N, a.px1, a.n, a.d, ks.scale, center, a.rw,
-        tgt, pl.n_tpad, src, pl.m_pad, Op::PP, Op::NS, W);
+        tgt, pl.n_tpad, src, pl.m_pad, Op::PP, NT, Op::NS, W);
     const int nb = combine_blocks(a.n);
     for (int t = T - 1; t >= 0; --t) {
         LDDMM_TRY(launch_single<Op>(pl, a.n, P, part, st));
-        cov_combine_kernel<Real><<<nb, kCombineThreads, 0, st>>>(
+        cov_combine_kernel<Real, DUP><<<nb, kCombineThreads, 0, st>>>(
             part, a.n, a.d, D, pl.split, dt, ks.dscale, a.rw, a.pxt + (long long)(t + 1) * N,
             a.at + (long long)t * N, a.pxt + (long long)t * N, a.dat ? a.dat + (long long)t * N : nullptr,
             t > 0 ? a.xt + (long long)(t - 1) * N : nullptr, t > 0 ? a.at + (long long)(t - 1) * N : nullptr,
@@ -328,6 +372,7 @@ template <class Real_, int KIND, int PDEG, int QDEG, int D>
 struct OpEPDiff {
     using Real = Real_;
     static constexpr bool F32 = sizeof(Real) == 4;
+    static constexpr int TPS = 1;
     static constexpr int BLOCK = 128, R = 2, TILE = 128, FOLD = F32 ? 32 : TILE;
     static constexpr int PP = PointPlanes<Real>::N;
     static constexpr int WP = (D + Traits<Real>::PER_WORD - 1) / Traits<Real>::PER_WORD;

@@ -34,16 +34,21 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
     const int tile_lo = (int)(((long long)chunk * sg.n_src_tiles) / sg.split);
     const int tile_hi = (int)(((long long)(chunk + 1) * sg.n_src_tiles) / sg.split);
 
-    // targets owned by this thread: t = tb*BLOCK*R + r*BLOCK + threadIdx.x (rows are padded)
-    typename Op::Tgt tg[R];
+    // targets owned by this thread: t = tb*BLOCK*R + r*BLOCK + threadIdx.x (rows are padded);
+    // an operator with TPS == 2 keeps two of them per slot (packed FP32 pairs)
+    constexpr int TPS = Op::TPS;
+    constexpr int SLOTS = R / TPS;
+    static_assert(R % TPS == 0, "R must be a multiple of TPS");
+    typename Op::Tgt tg[SLOTS];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        long long row = sg.tgt + (long long)tb * BLOCK * R + r * BLOCK + threadIdx.x;
-        Op::load_target(P, row, tg[r]);
+    for (int q = 0; q < SLOTS; ++q) {
+        const long long row = sg.tgt + (long long)tb * BLOCK * R + (q * TPS) * BLOCK + threadIdx.x;
+        if constexpr (TPS == 1) Op::load_target(P, row, tg[q]);
+        else Op::load_target(P, row, row + BLOCK, tg[q]);
     }
-    typename Op::Acc acc[R];
+    typename Op::Acc acc[SLOTS];
 #pragma unroll
-    for (int r = 0; r < R; ++r) acc[r].zero();
+    for (int q = 0; q < SLOTS; ++q) acc[q].zero();
 
     // global source words: Op lays a record out as NS planes of float4 words,
     // plane p of record j at P.src4[p * P.src_stride + j]
@@ -72,27 +77,33 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
 #pragma unroll 1
         for (int j0 = 0; j0 < TILE; j0 += Op::FOLD) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) acc[r].begin_fold();
+            for (int q = 0; q < SLOTS; ++q) acc[q].begin_fold();
 #pragma unroll 4
             for (int j = j0; j < j0 + Op::FOLD; ++j) {
                 typename Op::Src s;
                 Op::load_source(S, j, s);
 #pragma unroll
-                for (int r = 0; r < R; ++r) Op::pair(P, tg[r], s, acc[r]);
+                for (int q = 0; q < SLOTS; ++q) Op::pair(P, tg[q], s, acc[q]);
             }
 #pragma unroll
-            for (int r = 0; r < R; ++r) acc[r].end_fold();
+            for (int q = 0; q < SLOTS; ++q) acc[q].end_fold();
         }
         __syncthreads();
     }
 
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int t = tb * BLOCK * R + r * BLOCK + threadIdx.x;
-        if (t < sg.n_tgt) {
-            double* dst = part + (sg.part + (long long)chunk * sg.n_tgt + t) * NOUT;
+    for (int q = 0; q < SLOTS; ++q) {
 #pragma unroll
-            for (int c = 0; c < NOUT; ++c) dst[c] = acc[r].value(c);
+        for (int lane = 0; lane < TPS; ++lane) {
+            const int t = tb * BLOCK * R + (q * TPS + lane) * BLOCK + threadIdx.x;
+            if (t < sg.n_tgt) {
+                double* dst = part + (sg.part + (long long)chunk * sg.n_tgt + t) * NOUT;
+#pragma unroll
+                for (int c = 0; c < NOUT; ++c) {
+                    if constexpr (TPS == 1) dst[c] = acc[q].value(c);
+                    else dst[c] = acc[q].value(c, lane);
+                }
+            }
         }
     }
 }
