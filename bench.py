@@ -13,6 +13,16 @@ i.e. 4 * N * M target-source pairs.  Metric: kernel-sum pairs/s (whole job).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Other configurations (one JSON line each, not the default bench line):
+    --workload curve    2-D curve matching: 256-vertex ellipse -> bumped target,
+                        Gaussian sigma 0.5, current sigma 0.5, T = 10, 50 cg iterations
+    --workload surface  3-D surface matching: icosphere 10,242 vertices / 20,480
+                        faces -> 8-bump target, Gaussian sigma 0.2, varifold sigma
+                        0.1, T = 10, 100 cg iterations
+    --workload adjoint  gradient of the shooting + current objective on a
+                        163,842-vertex icosphere, T = 20, checkpoint every 5 steps,
+                        checked against central differences in FP64
+
 Multi-GPU (torchrun): each rank sweeps its own seeded instance (weak scaling,
 no data-path collective); the time is the max over ranks.
 The reference arm (--impl reference) times the reference algorithm's CPU
@@ -53,6 +63,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=16.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="kernels", choices=["kernels", "curve", "surface", "adjoint", "serving"])
+    ap.add_argument("--iters", type=int, default=None, help="cg iterations for the matching workloads")
+    ap.add_argument("--requests", type=int, default=512, help="requests of the serving stream")
+    ap.add_argument("--sigma-error", type=float, default=None, help="sigmaError of the matching workloads")
+    ap.add_argument("--max-active", type=int, default=64, help="serving slots")
     return ap.parse_args()
 
 
@@ -221,8 +236,474 @@ def measure_peaks(torch, lib, dev):
     return res
 
 
+# ---------------------------------------------------------------------------
+# matching workloads
+# ---------------------------------------------------------------------------
+def curve_problem(seed=3):
+    from registration_b200 import geometry as geo
+    rng = np.random.default_rng(seed)
+    v, f = geo.ellipse_curve(256, 1.0, 0.6)
+    vt, _ = geo.bumped_curve(v, 4, 0.3, 0.1, rng, n_out=256)
+    return v, vt
+
+
+def surface_problem(subdiv=5, n_bumps=8, width=0.25, amp=0.15, seed=5):
+    from registration_b200 import geometry as geo
+    rng = np.random.default_rng(seed)
+    v, f = geo.icosphere(subdiv)
+    vt = geo.bumped_sphere(v, f, n_bumps, width, amp, rng)
+    return v, f, vt
+
+
+def _line(args, metric, value, unit, higher, config, extra, dtype="f32 (compensated), f64 energies"):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+         "warmup": args.warmup, "higher_is_better": higher, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+         "data": "synthetic, seeded", "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_curve(args):
+    import logging
+    logging.disable(logging.INFO)
+    iters = args.iters or 50
+    v, vt = curve_problem()
+    config = {"workload": "curve matching: ellipse 256 vertices, gauss sigma 0.5, current sigma 0.5, sigmaError 1, "
+                          "T 10, %d cg iterations" % iters}
+    if args.impl == "reference":
+        import oracle
+        from oracle import lddmm_ref as ref
+        oracle.build()
+        oracle.set_num_threads(os.cpu_count() or 1)
+        times, objs = [], []
+        for s_ in range(max(1, args.warmup) + args.steps):
+            param = ref.MatchingParam(timeStep=0.1, KparDiff=ref.Kernel(name="gauss", sigma=0.5),
+                                      KparDist=ref.Kernel(name="gauss", sigma=0.5), sigmaError=1.0,
+                                      errorType="current", curves=True)
+            cm = ref.CurveMatching(ref.Curve(pointSet=v), ref.Curve(pointSet=vt), param, maxIter=iters)
+            t0 = time.perf_counter()
+            cm.optimizeMatching()
+            if s_ >= max(1, args.warmup):
+                times.append(time.perf_counter() - t0)
+                objs.append(cm.obj)
+        val = 1.0 / float(np.mean(times))
+        _line(args, "curve matches/s", val, "matches/s", True, config,
+              {"impl": "reference", "ms_per_step": 1e3 * float(np.mean(times)), "final_energy": objs[-1],
+               "cpu_baseline": {"value": val, "unit": "matches/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": "whole match"},
+               "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}},
+              dtype="f64")
+        return 0
+    import torch
+    from registration_b200 import curveMatching as CM
+    from registration_b200 import curves as cv
+    from registration_b200 import kernelFunctions as kf
+
+    def match(precision):
+        param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
+                                      KparDist=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
+                                      sigmaError=1.0, errorType="current")
+        cm = CM.CurveMatching(Template=cv.Curve(pointSet=v), Target=cv.Curve(pointSet=vt), param=param,
+                              maxIter=iters, saveRate=0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cm.optimizeMatching()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, cm
+
+    for _ in range(max(1, args.warmup)):
+        match("fp32c")
+    times = []
+    for _ in range(args.steps):
+        dt_, cm = match("fp32c")
+        times.append(dt_)
+    _, cm64 = match("fp64")
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        from oracle import lddmm_ref as ref
+        oracle.build()
+        oracle.set_num_threads(os.cpu_count() or 1)
+        param = ref.MatchingParam(timeStep=0.1, KparDiff=ref.Kernel(name="gauss", sigma=0.5),
+                                  KparDist=ref.Kernel(name="gauss", sigma=0.5), sigmaError=1.0, errorType="current",
+                                  curves=True)
+        rcm = ref.CurveMatching(ref.Curve(pointSet=v), ref.Curve(pointSet=vt), param, maxIter=iters)
+        t0 = time.perf_counter()
+        rcm.optimizeMatching()
+        tc = time.perf_counter() - t0
+        cpu = {"value": 1.0 / tc, "unit": "matches/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": "one whole match (FP64 numpy + C/OpenMP loops)", "final_energy": rcm.obj}
+    val = 1.0 / float(np.mean(times))
+    _line(args, "curve matches/s", val, "matches/s", True, config,
+          {"ms_per_step": 1e3 * float(np.mean(times)), "final_energy_fp32c": cm.obj, "final_energy_fp64": cm64.obj,
+           "final_energy_abs_diff": abs(cm.obj - cm64.obj), "iterations": cm.iter, "calls": cm.calls,
+           "cpu_baseline": cpu,
+           "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": int(v.nbytes + vt.nbytes),
+                   "d2h_bytes_per_step": int(cm.at.numel() * 8)}})
+    return 0
+
+
+def run_surface(args):
+    import logging
+    logging.disable(logging.INFO)
+    iters = args.iters or 100
+    v, f, vt = surface_problem()
+    config = {"workload": "surface matching: icosphere %d vertices / %d faces, 8 bumps, gauss sigma 0.2, varifold "
+                          "sigma 0.1, sigmaError 1, T 10, %d cg iterations" % (len(v), len(f), iters)}
+    import torch
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+
+    def match(precision, maxit):
+        param = SM.SurfaceMatchingParam(timeStep=0.1,
+                                        KparDiff=kf.Kernel(name="gauss", sigma=0.2, precision=precision),
+                                        KparDist=kf.Kernel(name="gauss", sigma=0.1, precision=precision),
+                                        sigmaError=1.0, errorType="varifold")
+        sm = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v]), Target=sf.Surface(FV=[f, vt]), param=param,
+                                maxIter=maxit, testGradient=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sm.optimizeMatching()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, sm
+
+    match("fp32c", 3)   # warm-up (library load, workspaces)
+    times = []
+    for _ in range(args.steps):
+        dt_, sm = match("fp32c", iters)
+        times.append(dt_)
+    t64, sm64 = match("fp64", iters)
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = surface_cpu_estimate(v, f, vt, sm.calls)
+    val = 1.0 / float(np.mean(times))
+    _line(args, "surface matches/s", val, "matches/s", True, config,
+          {"ms_per_step": 1e3 * float(np.mean(times)), "ms_per_iteration": 1e3 * float(np.mean(times)) / max(1, sm.iter),
+           "final_energy_fp32c": sm.obj, "final_energy_fp64": sm64.obj,
+           "final_energy_abs_diff": abs(sm.obj - sm64.obj), "iterations": sm.iter, "iterations_fp64": sm64.iter,
+           "fp64_gpu_ms": 1e3 * t64, "calls": sm.calls, "cpu_baseline": cpu,
+           "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": int(v.nbytes + vt.nbytes + f.nbytes),
+                   "d2h_bytes_per_step": int(sm.at.numel() * 8)}})
+    return 0
+
+
+def surface_cpu_estimate(v, f, vt, calls, sigma_def=0.2, sigma_dist=0.1, T=10):
+    """CPU time of one match extrapolated from timed single calls of the FP64
+    C/OpenMP oracle: updateTry = shot (T applyk) + varifold value (per pair,
+    no F x F arrays), getGradient = varifold gradient + adjoint (T applykdifft),
+    dotProduct = T applyk.  The reference's own numpy varifold would build
+    F x F x 3 FP64 arrays (10 GB each at F = 20,480)."""
+    import oracle
+    oracle.build()
+    oracle.set_num_threads(os.cpu_count() or 1)
+    c1 = (v[f[:, 0]] + v[f[:, 1]] + v[f[:, 2]]) / 3
+    s1 = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    a1 = np.sqrt((s1 ** 2).sum(1) + 1e-10)
+    n1 = s1 / a1[:, None]
+    a = 0.01 * np.random.default_rng(0).standard_normal(v.shape)
+    t0 = time.perf_counter()
+    oracle.applyk(v, v, a, sigma_def, 10)
+    t_k = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.varifold_pairs(c1, n1, a1, np.vstack([c1, c1]), np.vstack([n1, n1]), np.concatenate([a1, -a1]), sigma_dist,
+                          10, want=("val",))
+    t_val = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.varifold_pairs(c1, n1, a1, np.vstack([c1, c1]), np.vstack([n1, n1]), np.concatenate([a1, -a1]), sigma_dist,
+                          10, want=("z", "dz"))
+    t_grad = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.applykdifft(v, v, np.stack([a, a, a]), np.stack([a, a, a]), sigma_def, 10)
+    t_dkt = time.perf_counter() - t0
+    per_update = T * t_k + t_val
+    per_grad = t_grad + T * t_dkt
+    per_dot = T * t_k
+    total = calls["updateTry"] * per_update + calls["getGradient"] * per_grad + calls["dotProduct"] * per_dot
+    return {"value": 1.0 / total, "unit": "matches/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "per-call timings of the FP64 C/OpenMP oracle (applyk %.3fs, varifold value %.3fs, "
+                      "varifold gradient %.3fs, applykdifft na=3 %.3fs) x the GPU run's call counts %s"
+                      % (t_k, t_val, t_grad, t_dkt, calls),
+            "seconds_per_match": total}
+
+
+def run_adjoint(args):
+    import torch
+    from registration_b200 import autograd as ag
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaces as sf
+    v, f, vt = surface_problem(subdiv=7, n_bumps=32, width=0.1, amp=0.15, seed=9)
+    T = 20
+    rng = np.random.default_rng(1)
+    at = torch.from_numpy(0.002 * rng.standard_normal((T, len(v), 3))).cuda()
+    x0 = torch.from_numpy(v).cuda()
+    tmpl, tgt = sf.Surface(FV=[f, v]), sf.Surface(FV=[f, vt])
+
+    def geom(precision):
+        return ag.Geometry(tmpl, tgt, kf.Kernel(name="gauss", sigma=0.05, precision=precision),
+                           kf.Kernel(name="gauss", sigma=0.02, precision=precision), "current", sigmaError=1.0)
+
+    g32 = geom("fp32c")
+
+    def fwd_bwd(g):
+        a = at.clone().requires_grad_(True)
+        E = ag.lddmm_objective(a, x0, g, checkpoint_every=5)
+        E.backward()
+        return E, a.grad
+
+    for _ in range(max(1, args.warmup)):
+        fwd_bwd(g32)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        E, grad = fwd_bwd(g32)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    # FP64 objective + gradient, central differences (step 1e-3 on unit-norm directions)
+    g64 = geom("fp64")
+    E64, grad64 = fwd_bwd(g64)
+    fd = []
+    for k in range(2):
+        d = torch.from_numpy(rng.standard_normal(tuple(at.shape))).cuda()
+        d = d / d.norm()
+        h = 1e-3
+        ep = float(ag.lddmm_objective(at + h * d, x0, g64))
+        em = float(ag.lddmm_objective(at - h * d, x0, g64))
+        num = (ep - em) / (2 * h)
+        an64 = float((grad64 * d).sum())
+        an32 = float((grad * d).sum())
+        fd.append({"central_difference": num, "adjoint_fp64": an64, "adjoint_fp32c": an32,
+                   "rel_err_fp64": abs(num - an64) / abs(num), "rel_err_fp32c": abs(num - an32) / abs(num)})
+    n = len(v)
+    pairs = T * n * n * 3 + 2 * len(f) * 2 * len(f)   # shoot + re-shoot + adjoint sweeps, data value + gradient
+    config = {"workload": "adjoint: icosphere %d vertices / %d faces, 32 bumps, gauss sigma 0.05, current sigma "
+                          "0.02, T 20, checkpoint every 5 steps" % (n, len(f))}
+    val = 1.0 / float(np.mean(times))
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        oracle.build()
+        oracle.set_num_threads(os.cpu_count() or 1)
+        rows = 2048
+        t0 = time.perf_counter()
+        oracle.applyk(v[:rows], v, at[0].cpu().numpy(), 0.05, 10)
+        t_rows = time.perf_counter() - t0
+        t_k = t_rows * n / rows
+        cpu_s = T * t_k * 3 * 1.5   # forward, re-shoot, adjoint (applykdifft ~1.5x applyk), data term excluded
+        cpu = {"value": 1.0 / cpu_s, "unit": "gradients/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": "applyk on %d rows x %d sources (%.3fs), scaled by %d/%d rows, x 3 T sweeps x 1.5 "
+                         "(data term not counted)" % (rows, n, t_rows, n, rows)}
+    _line(args, "objective+gradient evaluations/s", val, "gradients/s", True, config,
+          {"ms_per_step": 1e3 * float(np.mean(times)), "energy_fp32c": float(E), "energy_fp64": float(E64),
+           "fd_checks": fd, "approx_pairs_per_step": pairs, "cpu_baseline": cpu,
+           "e2e": {"value": val, "unit": "gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8}})
+    return 0
+
+
+ICO_LEVELS = (3, 4, 5, 6, 7)
+
+
+def _serving_geometry(job):
+    """(seed, index, V, n_bumps) -> template vertices / faces and bumped target."""
+    from registration_b200 import geometry as geo
+    seed, i, V, nb = job
+    rng = np.random.default_rng([seed, i])
+    lvl = next(l for l in ICO_LEVELS if 10 * 4 ** l + 2 >= V)
+    cache = _serving_geometry.__dict__.setdefault("spheres", {})
+    if lvl not in cache:
+        cache[lvl] = geo.icosphere(lvl)
+    v, f = cache[lvl]
+    if V < len(v):
+        v, f = geo.decimate(v, f, V, rng)
+    vt = geo.bumped_sphere(v, f, nb, 0.25, 0.15, rng)
+    return v, f, vt
+
+
+def serving_stream(n_req, seed, iters, sigma_error):
+    """The request stream: icosphere-derived surfaces with V ~ logU[2000, 50000]
+    (smallest subdivision with at least V vertices, then random edge-collapse
+    decimation), target = 4-16 Gaussian bumps (width 0.25, amplitude 0.15),
+    deformation sigma ~ U[0.05, 0.3], varifold sigma = sigma / 2, T = 10.
+    The meshes are built in a spawned process pool (before any CUDA call)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import serving
+    from registration_b200 import surfaces as sf
+    from registration_b200.surfaceMatching import SurfaceMatchingParam
+    rng = np.random.default_rng(seed)
+    Vs = np.round(np.exp(rng.uniform(np.log(2000), np.log(50000), n_req))).astype(int)
+    nbs = rng.integers(4, 17, n_req)
+    sds = rng.uniform(0.05, 0.3, n_req)
+    jobs = [(seed, i, int(Vs[i]), int(nbs[i])) for i in range(n_req)]
+    # largest meshes first so that the pool's tail is short
+    order = sorted(range(n_req), key=lambda i: -Vs[i])
+    workers = max(1, min(16, (os.cpu_count() or 1)))
+    geo_out = [None] * n_req
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        for i, g in zip(order, ex.map(_serving_geometry, [jobs[i] for i in order])):
+            geo_out[i] = g
+    reqs = []
+    for i in range(n_req):
+        v, f, vt = geo_out[i]
+        sd = float(sds[i])
+        param = SurfaceMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=sd, precision="fp32c"),
+                                     KparDist=kf.Kernel(name="gauss", sigma=sd / 2, precision="fp32c"),
+                                     sigmaError=sigma_error, errorType="varifold")
+        reqs.append(serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[f, vt]), param, maxIter=iters,
+                                         rid=i))
+    return reqs
+
+
+def _fresh(reqs):
+    from registration_b200 import serving
+    from registration_b200 import surfaces as sf
+    return [serving.MatchRequest(sf.Surface(FV=[r.f0, r.v0]), sf.Surface(FV=[r.f1, r.v1]), r.param,
+                                 maxIter=r.max_iter, rid=r.rid) for r in reqs]
+
+
+def run_serving(args):
+    """Continuous batching of the request stream on one GPU.
+
+    1. capacity: the first min(64, R) requests served closed-loop (all at t=0);
+    2. the R-request stream with Poisson arrivals at 80% of that capacity:
+       throughput = R / (last finish - first arrival), latency = finish - arrival;
+    3. one-at-a-time FP64 GPU solves (SurfaceMatching, FP64 kernels, FP64
+       line search) of six requests spread over the size range, a few cg
+       iterations each: per-iteration time fitted as a + b V^2 and summed over
+       the stream with the served run's own iteration counts."""
+    import logging
+    logging.disable(logging.INFO)
+    import torch
+    from registration_b200 import serving
+    iters = args.iters or 50
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.1
+    R = args.requests
+    t_prep = time.perf_counter()
+    stream = serving_stream(R, args.seed, iters, sig_err)
+    t_prep = time.perf_counter() - t_prep
+    sizes = np.array([r.n for r in stream])
+    config = {"workload": "served surface matching: %d requests, V ~ logU[2000, 50000] icosphere-derived, 4-16 "
+                          "bumps, gauss sigma ~ U[0.05, 0.3], varifold sigma = sigma/2, sigmaError %g, T 10, %d cg "
+                          "iterations max, Poisson arrivals at 80%% of measured capacity, %d slots, 150 GB HBM "
+                          "budget" % (R, sig_err, iters, args.max_active)}
+    # warm-up: library load, workspace growth, cuBLAS handles
+    warm = _fresh([stream[int(np.argmin(sizes))]])
+    for r in warm:
+        r.max_iter = 2
+    serving.serve(warm, max_active=args.max_active)
+    torch.cuda.synchronize()
+    # 1. capacity, closed loop
+    ncal = min(64, R)
+    cal = _fresh(stream[:ncal])
+    t0 = time.perf_counter()
+    serving.serve(cal, max_active=args.max_active)
+    torch.cuda.synchronize()
+    cap = ncal / (time.perf_counter() - t0)
+    # 2. open loop at 80% of capacity
+    reqs = _fresh(stream)
+    rng = np.random.default_rng(args.seed + 1)
+    gaps = rng.exponential(1.0 / (0.8 * cap), size=R)
+    clocks = ClockSampler(gpu_id_for(0))
+    clocks.start()
+    t_start = time.perf_counter() + 0.05
+    arr = t_start + np.cumsum(gaps) - gaps[0]
+    for r, a in zip(reqs, arr):
+        r.arrival = float(a)
+    eng = serving.serve(reqs, max_active=args.max_active)
+    torch.cuda.synchronize()
+    t_end = max(r.finish for r in reqs)
+    clk = clocks.stop()
+    span = t_end - t_start
+    st = eng.stats()
+    ok = [r for r in reqs if r.error is None]
+    lat = np.array([r.latency() for r in ok])
+    its = np.array([r.result["iters"] for r in ok])
+    thr = len(ok) / span
+    # 3. one-at-a-time FP64 GPU solves of six requests across the size range
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+    order = np.argsort(sizes)
+    pick = [int(order[int(q * (R - 1))]) for q in (0.0, 0.2, 0.4, 0.6, 0.8, 1.0)]
+    base_it = 3
+    samples = []
+    for idx in pick:
+        r = stream[idx]
+        p = r.param
+
+        def solve(maxit):
+            param = SM.SurfaceMatchingParam(
+                timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=p.KparDiff.sigma, precision="fp64"),
+                KparDist=kf.Kernel(name="gauss", sigma=p.KparDist.sigma, precision="fp64"),
+                sigmaError=p.sigmaError, errorType="varifold")
+            sm = SM.SurfaceMatching(Template=sf.Surface(FV=[r.f0, r.v0]), Target=sf.Surface(FV=[r.f1, r.v1]),
+                                    param=param, maxIter=maxit, testGradient=False, verb=False,
+                                    lineSearchPrecision="fp64")
+            torch.cuda.synchronize()
+            ta = time.perf_counter()
+            sm.optimizeMatching()
+            torch.cuda.synchronize()
+            return time.perf_counter() - ta, sm
+
+        t1, sm1 = solve(1)
+        tk, smk = solve(base_it)
+        per_it = (tk - t1) / max(1, smk.iter - sm1.iter) if smk.iter > sm1.iter else tk / max(1, smk.iter)
+        samples.append({"V": int(r.n), "seconds_1_iter": t1, "seconds_%d_iter" % base_it: tk,
+                        "iters": int(smk.iter), "seconds_per_iter": per_it, "setup_seconds": max(0.0, t1 - per_it)})
+    Vs = np.array([s_["V"] for s_ in samples], dtype=np.float64)
+    A = np.stack([np.ones_like(Vs), Vs ** 2], axis=1)
+    coef_it, *_ = np.linalg.lstsq(A, np.array([s_["seconds_per_iter"] for s_ in samples]), rcond=None)
+    coef_set, *_ = np.linalg.lstsq(A, np.array([s_["setup_seconds"] for s_ in samples]), rcond=None)
+    it_by_rid = {r.rid: r.result["iters"] for r in ok}
+    pred = sum(max(0.0, coef_set[0] + coef_set[1] * n ** 2)
+               + max(1, it_by_rid.get(r.rid, iters)) * max(0.0, coef_it[0] + coef_it[1] * n ** 2)
+               for r, n in zip(stream, sizes))
+    base_thr = R / pred
+    # CPU: the FP64 C/OpenMP oracle's per-call timings on the median request x its served call counts
+    cpu = None
+    if not args.no_cpu_baseline:
+        mid = stream[int(order[R // 2])]
+        served = next((r for r in ok if r.rid == mid.rid), None)
+        if served is not None:
+            c = served.result["calls"]
+            calls = {"updateTry": c["value"], "getGradient": c["grad"], "dotProduct": c["dot"]}
+            cpu = surface_cpu_estimate(mid.v0, mid.f0, mid.v1, calls, mid.param.KparDiff.sigma,
+                                       mid.param.KparDist.sigma, mid.T)
+            cpu["sample"] = "median request (V=%d): " % mid.n + cpu["sample"]
+    h2d = int(sum(r.v0.nbytes + r.v1.nbytes + r.f0.nbytes + r.f1.nbytes for r in ok))
+    d2h = int(sum(r.result["at"].numel() * 8 for r in ok))
+    _line(args, "served surface matches/s", thr, "matches/s", True, config,
+          {"ms_per_step": 1e3 * span / max(1, len(ok)), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+           "p99_ms": 1e3 * float(np.percentile(lat, 99)), "capacity_closed_loop": cap,
+           "offered_rate": 0.8 * cap, "span_s": span, "failed": st["failed"], "rounds": st["rounds"],
+           "mean_batch": st["mean_batch"], "max_batch": st["max_batch"], "max_active": st["max_active"],
+           "iterations_mean": float(its.mean()), "iterations_min": int(its.min()),
+           "converged": int(sum(r.result["converged"] for r in ok)),
+           "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
+           "one_at_a_time_fp64_gpu": {"matches_per_s": base_thr, "seconds_per_stream": pred,
+                                      "per_iter_fit_s": [float(c_) for c_ in coef_it],
+                                      "setup_fit_s": [float(c_) for c_ in coef_set], "samples": samples},
+           "speedup_vs_one_at_a_time_fp64": thr / base_thr, "prep_seconds": t_prep, "clocks": clk,
+           "cpu_baseline": cpu,
+           "e2e": {"value": thr, "unit": "matches/s", "h2d_bytes_per_step": h2d // max(1, len(ok)),
+                   "d2h_bytes_per_step": d2h // max(1, len(ok))}})
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "curve":
+        return run_curve(args)
+    if args.workload == "surface":
+        return run_surface(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
+    if args.workload == "serving":
+        return run_serving(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch

@@ -117,19 +117,21 @@ LDDMM_API int lddmm_applydiv_f64(const double* x, int64_t n, const double* y, in
 /* ---- geodesic shooting: pointEvolution.landmarkDirectEvolutionEuler ----------
  * Replaces the T-step Euler loop of py-lddmm/pointEvolution.py:666-730 (no
  * affine part, no optional outputs):
- *   xt[0] = x0,  xt[t+1] = xt[t] + dt K(xt[t], xt[t]) at[t],  dt = 1/T
- * and, if energy != NULL, writes energy[0] = sum_t rw dt <at[t], K(xt[t]) at[t]>,
+ *   xt[0] = x0,  xt[t+1] = xt[t] + dt K(xt[t], xt[t]) at[t]
+ * with dt = 1/T (the reference) when dt <= 0, or the given dt (a segment of a
+ * longer shot), and, if energy != NULL, writes
+ * energy[0] = sum_t rw dt <at[t], K(xt[t]) at[t]>,
  * the deformation cost of objectiveFunDef (py-lddmm/surfaceMatching.py:205-212,
  * curveMatching.py:168-173), from the same kernel sums.
  * x0 (n, d), at (T, n, d), xt (T+1, n, d); energy: one double on the device. */
 LDDMM_API size_t lddmm_shoot_f32c_workspace(int64_t n, int d, int T);
-LDDMM_API int lddmm_shoot_f32c(const double* x0, int64_t n, int d, const double* at, int T, double sigma, int order,
-                               double regweight, double* xt, double* energy, void* workspace, size_t workspace_bytes,
-                               lddmm_stream_t stream);
+LDDMM_API int lddmm_shoot_f32c(const double* x0, int64_t n, int d, const double* at, int T, double dt,
+                               double sigma, int order, double regweight, double* xt, double* energy,
+                               void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 LDDMM_API size_t lddmm_shoot_f64_workspace(int64_t n, int d, int T);
-LDDMM_API int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* at, int T, double sigma, int order,
-                              double regweight, double* xt, double* energy, void* workspace, size_t workspace_bytes,
-                              lddmm_stream_t stream);
+LDDMM_API int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* at, int T, double dt,
+                              double sigma, int order, double regweight, double* xt, double* energy,
+                              void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* ---- Hamiltonian adjoint: landmarkHamiltonianCovector / Gradient --------------
  * Replaces the backward loop of py-lddmm/pointEvolution.py:735-765 and the
@@ -138,15 +140,17 @@ LDDMM_API int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* 
  *   pxt[t] = pxt[t+1] + dt applyDiffKT(xt[t], [pxt[t+1], at[t], -2 rw at[t]],
  *                                             [at[t], pxt[t+1], at[t]]),
  *   dat[t] = 2 rw at[t] - pxt[t+1]          (dat may be NULL)
+ * dt <= 0 means 1/T (the reference); a positive dt runs a segment of a longer
+ * adjoint (checkpointed trajectories).
  * xt (T+1, n, d), at (T, n, d), px1 (n, d), pxt (T+1, n, d), dat (T, n, d). */
 LDDMM_API size_t lddmm_covector_f32c_workspace(int64_t n, int d, int T);
-LDDMM_API int lddmm_covector_f32c(const double* xt, int64_t n, int d, const double* at, int T, const double* px1,
-                                  double sigma, int order, double regweight, double* pxt, double* dat, void* workspace,
-                                  size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_covector_f32c(const double* xt, int64_t n, int d, const double* at, int T, double dt,
+                                  const double* px1, double sigma, int order, double regweight, double* pxt,
+                                  double* dat, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 LDDMM_API size_t lddmm_covector_f64_workspace(int64_t n, int d, int T);
-LDDMM_API int lddmm_covector_f64(const double* xt, int64_t n, int d, const double* at, int T, const double* px1,
-                                 double sigma, int order, double regweight, double* pxt, double* dat, void* workspace,
-                                 size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_covector_f64(const double* xt, int64_t n, int d, const double* at, int T, double dt,
+                                 const double* px1, double sigma, int order, double regweight, double* pxt,
+                                 double* dat, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* ---- EPDiff shooting: pointEvolution.landmarkEPDiff ---------------------------
  * Replaces py-lddmm/pointEvolution.py:599-658 (no affine / optional outputs):
@@ -192,6 +196,63 @@ LDDMM_API int lddmm_dataterm_f64(int cell_size, int norm, const double* vertices
                                  const double* tgt_vectors, int64_t nc2, double sigma, int order, double eps1,
                                  double eps2, double* energy, const int64_t* vertex_ptr, const int64_t* vertex_idx,
                                  double* px, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+
+/* ---- ragged launches: many independent problems in one launch ----------------
+ * No single counterpart in the reference (which solves one problem per process);
+ * each segment computes exactly what the single-problem entry point above
+ * computes for its own rows, with its own kernel width, and its results do not
+ * depend on the other segments of the launch (per-segment chunking and FP64
+ * reduction trees).  Offsets / sigma / regweight arrays are HOST arrays.
+ *
+ * Shooting / adjoint of nreq requests, request s owning points
+ * [v_off[s], v_off[s+1]) (v_off has nreq+1 entries, v_off[0] = 0):
+ *   x0 (v_off[nreq], d); at / dat: request s's (T, n_s, d) block at row T*v_off[s];
+ *   xt / pxt: request s's (T+1, n_s, d) block at row (T+1)*v_off[s];
+ *   px1: (v_off[nreq], d); energy[s] = rw_s dt sum_t <a_t, K(x_t) a_t>; dt = 1/T.
+ * (pointEvolution.py:666-817, surfaceMatching.py:187-221) */
+LDDMM_API size_t lddmm_ragged_shoot_f32c_workspace(int nreq, const int64_t* v_off, int d, int T, int order);
+LDDMM_API int lddmm_ragged_shoot_f32c(int nreq, const int64_t* v_off, int d, const double* x0, const double* at,
+                                      int T, const double* sigma, int order, const double* regweight, double* xt,
+                                      double* energy, void* workspace, size_t workspace_bytes,
+                                      lddmm_stream_t stream);
+LDDMM_API size_t lddmm_ragged_covector_f32c_workspace(int nreq, const int64_t* v_off, int d, int T, int order);
+LDDMM_API int lddmm_ragged_covector_f32c(int nreq, const int64_t* v_off, int d, const double* xt, const double* at,
+                                         int T, const double* px1, const double* sigma, int order,
+                                         const double* regweight, double* pxt, double* dat, void* workspace,
+                                         size_t workspace_bytes, lddmm_stream_t stream);
+/* applyK segments (kernelFunctions.py:161-179): segment s maps targets x rows
+ * [t_start[s], +t_count[s]) and sources y rows [s_start[s], +s_count[s]) with
+ * weights beta (rows aligned with y, dimb <= 4 columns) to f rows
+ * [sum_{r<s} t_count[r], +t_count[s]) (compact, in segment order). */
+LDDMM_API size_t lddmm_ragged_applyk_f32c_workspace(int nseg, const int64_t* t_count, const int64_t* s_count, int d,
+                                                    int dimb, int order);
+LDDMM_API int lddmm_ragged_applyk_f32c(int nseg, const int64_t* t_start, const int64_t* t_count,
+                                       const int64_t* s_start, const int64_t* s_count, int d, const double* x,
+                                       const double* y, const double* beta, int dimb, const double* sigma, int order,
+                                       double* f, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+/* Data terms of nreq requests (surfaces.py:1009-1276, curves.py:539-703):
+ * request s owns vertices [v_off[s], v_off[s+1]), cells [c_off[s], c_off[s+1])
+ * (entries are GLOBAL vertex indices) and target cells [c2_off[s], c2_off[s+1]);
+ * vertex_ptr (v_off[nreq]+1) / vertex_idx (c_off[nreq]*cell_size, entries
+ * global cell*cell_size+corner) is the concatenated incidence; energy[nreq]. */
+LDDMM_API size_t lddmm_ragged_dataterm_f32c_workspace(int nreq, int cell_size, int norm, const int64_t* v_off,
+                                                      const int64_t* c_off, const int64_t* c2_off, int d, int order,
+                                                      int want_energy, int want_grad);
+LDDMM_API int lddmm_ragged_dataterm_f32c(int nreq, int cell_size, int norm, const int64_t* v_off,
+                                         const int64_t* c_off, const int64_t* c2_off, const double* vertices, int d,
+                                         const int64_t* cells, const double* tgt_centers, const double* tgt_vectors,
+                                         const double* sigma, int order, double eps1, double eps2, double* energy,
+                                         const int64_t* vertex_ptr, const int64_t* vertex_idx, double* px,
+                                         void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API size_t lddmm_ragged_dataterm_f64_workspace(int nreq, int cell_size, int norm, const int64_t* v_off,
+                                                     const int64_t* c_off, const int64_t* c2_off, int d, int order,
+                                                     int want_energy, int want_grad);
+LDDMM_API int lddmm_ragged_dataterm_f64(int nreq, int cell_size, int norm, const int64_t* v_off,
+                                        const int64_t* c_off, const int64_t* c2_off, const double* vertices, int d,
+                                        const int64_t* cells, const double* tgt_centers, const double* tgt_vectors,
+                                        const double* sigma, int order, double eps1, double eps2, double* energy,
+                                        const int64_t* vertex_ptr, const int64_t* vertex_idx, double* px,
+                                        void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* ---- diagnostics ------------------------------------------------------------
  * No counterpart in the reference.  Launches `blocks` x `threads` threads that

@@ -36,12 +36,12 @@ SIGNATURES = {
     "lddmm_applydiv_f64": (_I, [_P, _I64, _P, _I64, _P, _I, _D, _I, _P, _P, _SZ, _P]),
     "lddmm_shoot_f32c_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_shoot_f64_workspace": (_SZ, [_I64, _I, _I]),
-    "lddmm_shoot_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _I, _D, _P, _P, _P, _SZ, _P]),
-    "lddmm_shoot_f64": (_I, [_P, _I64, _I, _P, _I, _D, _I, _D, _P, _P, _P, _SZ, _P]),
+    "lddmm_shoot_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _D, _I, _D, _P, _P, _P, _SZ, _P]),
+    "lddmm_shoot_f64": (_I, [_P, _I64, _I, _P, _I, _D, _D, _I, _D, _P, _P, _P, _SZ, _P]),
     "lddmm_covector_f32c_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_covector_f64_workspace": (_SZ, [_I64, _I, _I]),
-    "lddmm_covector_f32c": (_I, [_P, _I64, _I, _P, _I, _P, _D, _I, _D, _P, _P, _P, _SZ, _P]),
-    "lddmm_covector_f64": (_I, [_P, _I64, _I, _P, _I, _P, _D, _I, _D, _P, _P, _P, _SZ, _P]),
+    "lddmm_covector_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _P, _D, _I, _D, _P, _P, _P, _SZ, _P]),
+    "lddmm_covector_f64": (_I, [_P, _I64, _I, _P, _I, _D, _P, _D, _I, _D, _P, _P, _P, _SZ, _P]),
     "lddmm_dataterm_f32c_workspace": (_SZ, [_I, _I, _I64, _I, _I64, _I64, _I, _I, _I]),
     "lddmm_dataterm_f64_workspace": (_SZ, [_I, _I, _I64, _I, _I64, _I64, _I, _I, _I]),
     "lddmm_dataterm_f32c": (_I, [_I, _I, _P, _I64, _I, _P, _I64, _P, _P, _I64, _D, _I, _D, _D, _P, _P, _P, _P,
@@ -52,6 +52,19 @@ SIGNATURES = {
     "lddmm_epdiff_f64_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_epdiff_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _I, _P, _P, _P, _SZ, _P]),
     "lddmm_epdiff_f64": (_I, [_P, _I64, _I, _P, _I, _D, _I, _P, _P, _P, _SZ, _P]),
+    # ragged launches: offset / sigma / regweight arguments are host arrays
+    "lddmm_ragged_shoot_f32c_workspace": (_SZ, [_I, _P, _I, _I, _I]),
+    "lddmm_ragged_shoot_f32c": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _P, _SZ, _P]),
+    "lddmm_ragged_covector_f32c_workspace": (_SZ, [_I, _P, _I, _I, _I]),
+    "lddmm_ragged_covector_f32c": (_I, [_I, _P, _I, _P, _P, _I, _P, _P, _I, _P, _P, _P, _P, _SZ, _P]),
+    "lddmm_ragged_applyk_f32c_workspace": (_SZ, [_I, _P, _P, _I, _I, _I]),
+    "lddmm_ragged_applyk_f32c": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _P, _SZ, _P]),
+    "lddmm_ragged_dataterm_f32c_workspace": (_SZ, [_I, _I, _I, _P, _P, _P, _I, _I, _I, _I]),
+    "lddmm_ragged_dataterm_f64_workspace": (_SZ, [_I, _I, _I, _P, _P, _P, _I, _I, _I, _I]),
+    "lddmm_ragged_dataterm_f32c": (_I, [_I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _I, _D, _D, _P, _P, _P, _P,
+                                        _P, _SZ, _P]),
+    "lddmm_ragged_dataterm_f64": (_I, [_I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _I, _D, _D, _P, _P, _P, _P,
+                                       _P, _SZ, _P]),
 }
 
 ERRORS = {-1: "invalid argument", -2: "workspace too small", -3: "CUDA error", -4: "unsupported"}

@@ -65,6 +65,7 @@ class DeviceMatching:
         self.AfftTry = self.Afft
         self.xt = self.x0.unsqueeze(0).repeat(self.Tsize + 1, 1, 1)
         self.xtTry = None
+        self.calls = {"updateTry": 0, "getGradient": 0, "dotProduct": 0}
         self.obj = None
         self.objTry = None
         self.gradCoeff = self.npt
@@ -142,6 +143,7 @@ class DeviceMatching:
 
     def updateTry(self, dir, eps, objRef=None):
         """(surfaceMatching.py:255-289); NaN objectives return 1e500."""
+        self.calls["updateTry"] += 1
         atTry = self.at - eps * dir.diff
         xt, e = evol.shoot(self.x0, atTry, self.param.KparDiff, regweight=self.regweight, with_energy=True)
         objTry = self.obj0 + float(e + self._data_energy(xt[-1]))
@@ -156,6 +158,7 @@ class DeviceMatching:
 
     def getGradient(self, coeff=1.0):
         """(surfaceMatching.py:301-327): grd.diff = (2 rw a - p_{t+1}) / (coeff T)."""
+        self.calls["getGradient"] += 1
         px1 = -self.endPointGradient()
         _, dat = evol.covector(self.xt, self.at, px1, self.param.KparDiff, self.regweight, with_dat=True)
         grd = Direction()
@@ -183,6 +186,7 @@ class DeviceMatching:
 
     def dotProduct(self, g1, g2):
         """sum_t <g2_t, K(x_t) g1_t> (surfaceMatching.py:353-377), FP64 on the device."""
+        self.calls["dotProduct"] += 1
         acc = torch.zeros(len(g2), dtype=torch.float64, device=self.x0.device)
         K = self.param.KparDiff
         for t in range(self.Tsize):

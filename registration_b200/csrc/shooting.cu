@@ -179,6 +179,7 @@ struct ShootArgs {
     int d;
     const double* at;
     int T;
+    double dt;  // Euler step; <= 0 means 1/T
     double sigma;
     int order;
     double rw;
@@ -210,7 +211,7 @@ int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     bbox_center_kernel<<<1, 256, 0, st>>>(a.x0, a.n, nullptr, 0, a.d, center);
     shoot_pack_kernel<Real, DUP><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.x0, a.at, a.n, a.d, ks.scale, center, tgt, pl.n_tpad, src, pl.m_pad, Op::PP, D, Op::NS);
-    const double dt = 1.0 / a.T;
+    const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
     for (int t = 0; t < a.T; ++t) {
         LDDMM_TRY(launch_single<Op>(pl, a.n, P, part, st));
         shoot_combine_kernel<Real, DUP><<<nb, kCombineThreads, 0, st>>>(
@@ -308,6 +309,7 @@ struct CovArgs {
     int d;
     const double* at;
     int T;
+    double dt;  // Euler step; <= 0 means 1/T
     const double* px1;
     double sigma;
     int order;
@@ -336,7 +338,7 @@ int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     P.tgt_stride = pl.n_tpad;
     set_poly(P, ks);
     const long long N = a.n * a.d;
-    const double dt = 1.0 / a.T;
+    const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.pxt + (long long)a.T * N, a.px1, sizeof(double) * N,
                                          cudaMemcpyDeviceToDevice, st), "covector copy"));
     const int T = a.T;
@@ -652,34 +654,34 @@ extern "C" {
 size_t lddmm_shoot_f32c_workspace(int64_t n, int d, int T) { return shoot_ws<float>(n, d, T); }
 size_t lddmm_shoot_f64_workspace(int64_t n, int d, int T) { return shoot_ws<double>(n, d, T); }
 
-int lddmm_shoot_f32c(const double* x0, int64_t n, int d, const double* at, int T, double sigma, int order,
-                     double regweight, double* xt, double* energy, void* workspace, size_t workspace_bytes,
-                     lddmm_stream_t stream) {
-    ShootArgs a{x0, n, d, at, T, sigma, order, regweight, xt, energy};
+int lddmm_shoot_f32c(const double* x0, int64_t n, int d, const double* at, int T, double dt, double sigma,
+                     int order, double regweight, double* xt, double* energy, void* workspace,
+                     size_t workspace_bytes, lddmm_stream_t stream) {
+    ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
     return shoot_entry<float>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
-int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* at, int T, double sigma, int order,
-                    double regweight, double* xt, double* energy, void* workspace, size_t workspace_bytes,
-                    lddmm_stream_t stream) {
-    ShootArgs a{x0, n, d, at, T, sigma, order, regweight, xt, energy};
+int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* at, int T, double dt, double sigma,
+                    int order, double regweight, double* xt, double* energy, void* workspace,
+                    size_t workspace_bytes, lddmm_stream_t stream) {
+    ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
     return shoot_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 size_t lddmm_covector_f32c_workspace(int64_t n, int d, int T) { return cov_ws<float>(n, d, T); }
 size_t lddmm_covector_f64_workspace(int64_t n, int d, int T) { return cov_ws<double>(n, d, T); }
 
-int lddmm_covector_f32c(const double* xt, int64_t n, int d, const double* at, int T, const double* px1, double sigma,
-                        int order, double regweight, double* pxt, double* dat, void* workspace,
+int lddmm_covector_f32c(const double* xt, int64_t n, int d, const double* at, int T, double dt, const double* px1,
+                        double sigma, int order, double regweight, double* pxt, double* dat, void* workspace,
                         size_t workspace_bytes, lddmm_stream_t stream) {
-    CovArgs a{xt, n, d, at, T, px1, sigma, order, regweight, pxt, dat};
+    CovArgs a{xt, n, d, at, T, dt, px1, sigma, order, regweight, pxt, dat};
     return cov_entry<float>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
-int lddmm_covector_f64(const double* xt, int64_t n, int d, const double* at, int T, const double* px1, double sigma,
-                       int order, double regweight, double* pxt, double* dat, void* workspace,
+int lddmm_covector_f64(const double* xt, int64_t n, int d, const double* at, int T, double dt, const double* px1,
+                       double sigma, int order, double regweight, double* pxt, double* dat, void* workspace,
                        size_t workspace_bytes, lddmm_stream_t stream) {
-    CovArgs a{xt, n, d, at, T, px1, sigma, order, regweight, pxt, dat};
+    CovArgs a{xt, n, d, at, T, dt, px1, sigma, order, regweight, pxt, dat};
     return cov_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

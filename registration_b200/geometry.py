@@ -128,40 +128,53 @@ def bumped_curve(v, n_bumps, width, amp_std, rng, n_out=None):
 def decimate(v, f, target_vertices, rng):
     """Random edge collapse (midpoint) until ``target_vertices`` remain.
 
-    Collapses keep the mesh a valid triangle soup: faces that degenerate are
-    dropped and vertex indices are compacted at the end.  Orientation of the
-    surviving faces is unchanged."""
+    Each round proposes one random edge per face with a random priority and
+    collapses, all at once, the edges whose priority is the smallest within
+    the 1-rings of both end points (so simultaneous collapses never touch the
+    same triangles) and whose end points share exactly two neighbours (the
+    link condition: the surface stays a closed 2-manifold).  Faces that
+    degenerate are dropped and vertex indices are compacted at the end;
+    orientation of the surviving faces is unchanged."""
+    import scipy.sparse as sp
     v = v.copy()
-    f = f.copy()
-    alive = np.ones(len(v), dtype=bool)
-    remap = np.arange(len(v))
-    n_alive = len(v)
+    f = np.asarray(f, dtype=np.int64).copy()
+    nv = len(v)
+    alive = np.ones(nv, dtype=bool)
+    n_alive = nv
     while n_alive > target_vertices and len(f) > 4:
-        batch = max(1, min(n_alive - target_vertices, len(f) // 16))
-        picks = rng.choice(len(f), size=batch, replace=False)
-        used = np.zeros(len(v), dtype=bool)
-        for q in picks:
-            j = rng.integers(3)
-            a, b = f[q, j], f[q, (j + 1) % 3]
-            if a == b or used[a] or used[b]:
-                continue
-            used[a] = used[b] = True
-            v[a] = 0.5 * (v[a] + v[b])
-            alive[b] = False
-            remap[b] = a
-            n_alive -= 1
-            if n_alive <= target_vertices:
-                break
-        # resolve chains of collapses, rewrite and drop degenerate faces
-        while True:
-            nxt = remap[remap]
-            if np.array_equal(nxt, remap):
-                break
-            remap = nxt
+        rows = np.arange(len(f))
+        j = rng.integers(3, size=len(f))
+        a = f[rows, j]
+        b = f[rows, (j + 1) % 3]
+        pr = rng.random(len(f))
+        best = np.full(nv, np.inf)
+        np.minimum.at(best, a, pr)
+        np.minimum.at(best, b, pr)
+        fb = best[f].min(axis=1)
+        ring = np.full(nv, np.inf)
+        for c in range(3):
+            np.minimum.at(ring, f[:, c], fb)
+        sel = np.flatnonzero((ring[a] == pr) & (ring[b] == pr) & (a != b))
+        if sel.size:
+            e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+            adj = sp.csr_matrix((np.ones(len(e)), (e[:, 0], e[:, 1])), shape=(nv, nv))
+            adj = ((adj + adj.T) > 0).astype(np.float64)
+            common = np.asarray(adj[a[sel]].multiply(adj[b[sel]]).sum(axis=1)).ravel()
+            sel = sel[common == 2]
+        cap = n_alive - target_vertices
+        sel = sel[np.argsort(pr[sel], kind="stable")[:cap]]
+        if sel.size == 0:
+            break
+        a, b = a[sel], b[sel]
+        v[a] = 0.5 * (v[a] + v[b])
+        alive[b] = False
+        n_alive -= sel.size
+        remap = np.arange(nv)
+        remap[b] = a
         f = remap[f]
         keep = (f[:, 0] != f[:, 1]) & (f[:, 1] != f[:, 2]) & (f[:, 2] != f[:, 0])
         f = f[keep]
     idx = np.flatnonzero(alive)
-    new = -np.ones(len(v), dtype=np.int64)
+    new = -np.ones(nv, dtype=np.int64)
     new[idx] = np.arange(len(idx))
     return v[idx], new[f]

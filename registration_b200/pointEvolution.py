@@ -36,8 +36,9 @@ def _kernel_args(K):
     return float(K.sigma), int(K.order), _suffix(K.precision)
 
 
-def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False):
-    """Device call: returns (xt, energy) with energy = sum_t rw dt <a_t, K(x_t) a_t> (a 0-d tensor) or None."""
+def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False, dt=None):
+    """Device call: returns (xt, energy) with energy = sum_t rw dt <a_t, K(x_t) a_t> (a 0-d tensor) or None.
+    dt defaults to 1/T; pass it to shoot a segment of a longer trajectory."""
     require_cuda()
     x0d = to_dev(x0)
     atd = to_dev(at)
@@ -49,13 +50,13 @@ def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False):
     energy = torch.empty((), dtype=torch.float64, device=x0d.device) if with_energy else None
     wsb = _lib.query("lddmm_shoot_%s_workspace" % sfx, n, d, T)
     ws = workspace.get(wsb)
-    _lib.call("lddmm_shoot_" + sfx, ptr(x0d), n, d, ptr(atd), T, sigma, order, float(regweight), ptr(xt),
+    _lib.call("lddmm_shoot_" + sfx, ptr(x0d), n, d, ptr(atd), T, float(dt or 0.0), sigma, order, float(regweight), ptr(xt),
               ptr(energy) if energy is not None else None, ptr(ws), wsb, stream_handle())
     return xt, energy
 
 
-def covector(xt, at, px1, KparDiff, regweight, with_dat=True):
-    """Device call: returns (pxt, dat) given the trajectory xt (T+1, N, dim)."""
+def covector(xt, at, px1, KparDiff, regweight, with_dat=True, dt=None):
+    """Device call: returns (pxt, dat) given the trajectory xt (T+1, N, dim); dt defaults to 1/T."""
     require_cuda()
     xtd, atd, pxd = to_dev(xt), to_dev(at), to_dev(px1)
     T, n, d = atd.shape
@@ -64,7 +65,8 @@ def covector(xt, at, px1, KparDiff, regweight, with_dat=True):
     dat = torch.empty((T, n, d), dtype=torch.float64, device=xtd.device) if with_dat else None
     wsb = _lib.query("lddmm_covector_%s_workspace" % sfx, n, d, T)
     ws = workspace.get(wsb)
-    _lib.call("lddmm_covector_" + sfx, ptr(xtd), n, d, ptr(atd), T, ptr(pxd), sigma, order, float(regweight),
+    _lib.call("lddmm_covector_" + sfx, ptr(xtd), n, d, ptr(atd), T, float(dt or 0.0), ptr(pxd), sigma, order,
+              float(regweight),
               ptr(pxt), ptr(dat) if dat is not None else None, ptr(ws), wsb, stream_handle())
     return pxt, dat
 

@@ -1,0 +1,548 @@
+"""Continuous-batching server for surface / curve matching requests.
+
+Each request is a matching problem with the interface of
+py-lddmm/surfaceMatching.py:74-484 (or curveMatching.py:58-354): Euler
+shooting of the template, a current / measure / varifold data term and the
+conjugate-gradient loop of conjugateGradient.cg.  The optimiser of every
+request runs unchanged in its own host thread; the calls that do GPU work
+(objective and trial-step values, gradients, K-metric dot products) post a
+work item to the engine and wait for its result.  The engine loop:
+
+  1. admits arrived requests while the HBM budget and the slot count allow;
+     an admitted request's momenta, trajectories and optimiser directions
+     stay on the device until it finishes;
+  2. waits until every active request has posted its next work item;
+  3. runs each kind of pending work as ONE ragged launch over all requests
+     that posted it (lddmm_ragged_* entry points: segment tables with
+     per-request offsets, kernel widths and source-chunk counts);
+  4. hands the results back and repeats.
+
+Requests that arrive while others are on the GPU are admitted at once and join
+the next launches, so their work overlaps on the device.  Every per-request
+quantity (packing frame, source chunking, reduction trees, line-search
+decisions) depends only on that request's own data, so a request's result is
+bit-identical alone and in any mix.
+
+Precision: FP32 compensated kernel sums for shooting, the adjoint, the data
+term and the dot products; every energy and dot product is reduced in FP64 and
+the line search compares FP64 numbers.  ``line_search_precision='fp64'`` makes
+the data-term VALUES FP64 pair sums as well (the single-problem default, needed
+to reproduce the reference's iteration trace; it costs a full FP64 sweep per
+trial step).
+"""
+import ctypes
+import threading
+import time
+
+import numpy as np
+import torch
+
+from . import _dataterm as _dt
+from . import _lib
+from . import conjugateGradient as cg
+from .device import ptr, require_cuda, stream_handle, workspace
+
+NORMS = {"current": 0, "measure": 1, "varifold": 2}
+
+
+def _i64(a):
+    return (ctypes.c_int64 * len(a))(*[int(v) for v in a])
+
+
+def _f64(a):
+    return (ctypes.c_double * len(a))(*[float(v) for v in a])
+
+
+def _order(K):
+    return 10 if K.name == "gauss" else int(K.order)
+
+
+class MatchRequest:
+    """One matching problem.
+
+    Template / Target: surfaces.Surface or curves.Curve (vertices, faces);
+    param: SurfaceMatchingParam / CurveMatchingParam (timeStep, KparDiff,
+    KparDist, sigmaError, errorType); maxIter / regWeight as in
+    SurfaceMatching.  The kernels' sigma / name / order are used; the kernel
+    sums run in FP32 with compensated accumulation whatever their precision."""
+
+    def __init__(self, Template, Target, param, maxIter=50, regWeight=1.0, rid=None):
+        if param.errorType not in NORMS:
+            raise ValueError("errorType must be one of %s" % sorted(NORMS))
+        self.v0 = np.ascontiguousarray(np.asarray(Template.vertices, dtype=np.float64))
+        self.f0 = np.ascontiguousarray(np.asarray(Template.faces, dtype=np.int64))
+        self.v1 = np.ascontiguousarray(np.asarray(Target.vertices, dtype=np.float64))
+        self.f1 = np.ascontiguousarray(np.asarray(Target.faces, dtype=np.int64))
+        if self.f0.shape[1] != self.f1.shape[1] or self.v0.shape[1] != self.v1.shape[1]:
+            raise ValueError("template and target must have the same cell size and dimension")
+        if param.errorType == "varifold" and self.f0.shape[1] != 3:
+            raise ValueError("the varifold norm is defined for triangulated surfaces")
+        self.param = param
+        self.T = int(round(1.0 / param.timeStep))
+        self.max_iter = int(maxIter)
+        self.regweight = float(regWeight)
+        self.rid = rid
+        self.arrival = None
+        self.start = None
+        self.finish = None
+        self.result = None
+        self.error = None
+        self.done = threading.Event()
+
+    @property
+    def n(self):
+        return len(self.v0)
+
+    @property
+    def group(self):
+        """Requests of one group can share a ragged launch."""
+        p = self.param
+        return (self.v0.shape[1], self.f0.shape[1], p.errorType, _order(p.KparDiff), _order(p.KparDist), self.T)
+
+    def hbm_bytes(self):
+        """Resident device state: momenta, trial momenta, gradient and three
+        optimiser directions (T n d each), two trajectories and the adjoint
+        ((T+1) n d each), target cells and topology, plus a share of the
+        ragged launches' packed records."""
+        n, d, T = self.n, self.v0.shape[1], self.T
+        cells = len(self.f0) + len(self.f1)
+        return 8 * (7 * T * n * d + 4 * (T + 1) * n * d) + 160 * cells + 96 * n * (T + 2)
+
+    def latency(self):
+        return None if self.finish is None else self.finish - self.arrival
+
+
+class _Direction:
+    __slots__ = ("diff", "aff", "initx")
+
+    def __init__(self, diff):
+        self.diff = diff
+        self.aff = np.zeros((0,))
+        self.initx = []
+
+
+class _Problem:
+    """The optimiser protocol (surfaceMatching.py:233-377) of one request; the
+    GPU work is posted to the engine."""
+
+    def __init__(self, req, engine):
+        self.req = req
+        self.engine = engine
+        dev = engine.device
+        p = req.param
+        self.T = self.Tsize = req.T
+        self.dim = req.v0.shape[1]
+        self.npt = req.n
+        self.sigma_def = float(p.KparDiff.sigma)
+        self.sigma_dist = float(p.KparDist.sigma)
+        self.s2 = float(p.sigmaError) ** 2
+        self.x0 = torch.from_numpy(req.v0).to(dev)
+        self.v1 = torch.from_numpy(req.v1).to(dev)
+        c1, s1 = _dt.cell_geometry(req.v1, req.f1)
+        self.tc = torch.from_numpy(np.ascontiguousarray(c1)).to(dev)
+        self.tv = torch.from_numpy(np.ascontiguousarray(s1)).to(dev)
+        self.dshape = _dt.DeviceShape(req.f0, req.n)
+        self.tshape = _dt.DeviceShape(req.f1, len(req.v1))
+        self.at = torch.zeros((self.T, self.npt, self.dim), dtype=torch.float64, device=dev)
+        self.atTry = self.at
+        self.xt = self.x0.unsqueeze(0).repeat(self.T + 1, 1, 1)
+        self.xtTry = None
+        self.obj = None
+        self.objTry = None
+        self.obj0 = None
+        self.gradCoeff = self.npt
+        self.converged = False
+        self.iters = 0
+        self.calls = {"value": 0, "grad": 0, "dot": 0}
+
+    def getVariable(self):
+        return [self.at]
+
+    def objectiveFun(self):
+        if self.obj is None:
+            self.obj0 = self.engine.post(self, "norm0", None)
+            e, self.xt = self.engine.post(self, "value", self.at)
+            self.obj = e + self.obj0
+        return self.obj
+
+    def updateTry(self, dir, eps, objRef=None):
+        atTry = self.at - eps * dir.diff
+        e, xt = self.engine.post(self, "value", atTry)
+        objTry = self.obj0 + e
+        if np.isnan(objTry):
+            return 1e500
+        if (objRef is None) or (objTry < objRef):
+            self.atTry = atTry
+            self.objTry = objTry
+            self.xtTry = xt
+        return objTry
+
+    def getGradient(self, coeff=1.0):
+        dat = self.engine.post(self, "grad", None)
+        return _Direction(dat / (coeff * self.T))
+
+    def dotProduct(self, g1, g2):
+        return self.engine.post(self, "dot", (g1.diff, [g.diff for g in g2]))
+
+    def addProd(self, d1, d2, beta):
+        return _Direction(d1.diff + beta * d2.diff)
+
+    def copyDir(self, d0):
+        return _Direction(d0.diff.clone())
+
+    def acceptVarTry(self):
+        self.obj = self.objTry
+        self.at = self.atTry
+        if self.xtTry is not None:
+            self.xt = self.xtTry
+
+    def endOfIteration(self):
+        self.iters += 1
+
+
+class Scheduler:
+    """Admission, rounds and grouping of the continuous-batching loop.
+
+    Subclasses provide _make_problem(req) and one _do_<kind>(items) method per
+    kind of work ("norm0", "value", "grad", "dot"), each mapping a list of
+    (problem, payload) to a list of results (one launch per call).
+    hbm_budget_bytes: admission limit on the sum of the active requests'
+    resident state (MatchRequest.hbm_bytes); max_active: slot count."""
+
+    def __init__(self, hbm_budget_bytes=150e9, max_active=64):
+        self.hbm_budget = float(hbm_budget_bytes)
+        self.max_active = int(max_active)
+        self.cv = threading.Condition()
+        self.queue = []          # submitted, not admitted (sorted by arrival)
+        self.active = set()
+        self.pending = {}        # problem -> (kind, payload)
+        self.results = {}
+        self.events = {}
+        self.finished = []
+        self.hbm_in_use = 0.0
+        self.rounds = 0
+        self.launches = {"norm0": 0, "value": 0, "grad": 0, "dot": 0}
+        self.batch_sizes = []
+        self.busy_seconds = 0.0
+        self.max_active_seen = 0
+
+    # -- request side ------------------------------------------------------------------
+    def submit(self, req, arrival=None):
+        """Queues a request; `arrival` (perf_counter seconds) may lie in the future."""
+        req.arrival = time.perf_counter() if arrival is None else float(arrival)
+        with self.cv:
+            self.queue.append(req)
+            self.queue.sort(key=lambda r: r.arrival)
+            self.cv.notify_all()
+        return req
+
+    def post(self, prob, kind, payload):
+        ev = threading.Event()
+        with self.cv:
+            self.events[prob] = ev
+            self.pending[prob] = (kind, payload)
+            self.cv.notify_all()
+        ev.wait()
+        res = self.results.pop(prob)
+        if isinstance(res, BaseException):
+            raise res
+        return res
+
+    def _run_request(self, prob):
+        req = prob.req
+        try:
+            # SurfaceMatching.optimizeMatching (surfaceMatching.py:474-484)
+            grd = prob.getGradient(prob.gradCoeff)
+            [g2] = prob.dotProduct(grd, [grd])
+            prob.gradEps = max(0.001, np.sqrt(g2) / 10000)
+            cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False, epsInit=0.1)
+            req.result = {"at": prob.at, "xt": prob.xt, "obj": prob.obj, "iters": prob.iters,
+                          "converged": prob.converged, "calls": dict(prob.calls)}
+        except BaseException as exc:   # this request fails, the others go on
+            req.error = exc
+        finally:
+            req.finish = time.perf_counter()
+            with self.cv:
+                self.active.discard(prob)
+                self.hbm_in_use -= req.hbm_bytes()
+                self.finished.append(req)
+                self.cv.notify_all()
+            req.done.set()
+
+    # -- engine side -----------------------------------------------------------------
+    def _admit(self, now):
+        start = []
+        with self.cv:
+            keep = []
+            for req in self.queue:
+                if req.arrival > now:
+                    keep.append(req)
+                elif req.hbm_bytes() > self.hbm_budget:
+                    req.error = MemoryError("request needs %.3g bytes of device state; the budget is %.3g"
+                                            % (req.hbm_bytes(), self.hbm_budget))
+                    req.start = req.finish = now
+                    self.finished.append(req)
+                    req.done.set()
+                elif (len(self.active) + len(start) < self.max_active
+                      and self.hbm_in_use + req.hbm_bytes() <= self.hbm_budget):
+                    self.hbm_in_use += req.hbm_bytes()
+                    start.append(req)
+                else:
+                    keep.append(req)
+            self.queue = keep
+        for req in start:
+            req.start = time.perf_counter()
+            try:
+                prob = self._make_problem(req)
+            except BaseException as exc:
+                req.error = exc
+                req.finish = time.perf_counter()
+                with self.cv:
+                    self.hbm_in_use -= req.hbm_bytes()
+                    self.finished.append(req)
+                req.done.set()
+                continue
+            with self.cv:
+                self.active.add(prob)
+                self.max_active_seen = max(self.max_active_seen, len(self.active))
+            threading.Thread(target=self._run_request, args=(prob,), daemon=True).start()
+
+    def _can_admit(self, now):
+        if not self.queue or self.queue[0].arrival > now:
+            return False
+        req = self.queue[0]
+        return (len(self.active) < self.max_active
+                and (self.hbm_in_use + req.hbm_bytes() <= self.hbm_budget or req.hbm_bytes() > self.hbm_budget))
+
+    def run(self):
+        """Serves until the queue (including future arrivals) and the active set are empty."""
+        while True:
+            self._admit(time.perf_counter())
+            with self.cv:
+                if not self.active and not self.queue:
+                    return
+                ready = None
+                while True:
+                    if self.active and len(self.pending) == len(self.active):
+                        ready = self.pending
+                        self.pending = {}
+                        break
+                    now = time.perf_counter()
+                    if self._can_admit(now):
+                        break
+                    nxt = self.queue[0].arrival if self.queue else None
+                    if not self.active and nxt is None:
+                        break
+                    wait = None if (nxt is None or nxt <= now) else nxt - now
+                    self.cv.wait(timeout=wait)
+            if ready:
+                t0 = time.perf_counter()
+                self._execute(ready)
+                self.busy_seconds += time.perf_counter() - t0
+                self.rounds += 1
+
+    def _execute(self, ready):
+        groups = {}
+        for prob, (kind, payload) in ready.items():
+            groups.setdefault((kind, prob.req.group), []).append((prob, payload))
+        self.batch_sizes.append(len(ready))
+        out = {}
+        for (kind, _), items in groups.items():
+            self.launches[kind] += 1
+            fn = getattr(self, "_do_" + kind)
+            try:
+                res = fn(items)
+            except Exception as exc:
+                # isolate the failing request(s): re-run the group one by one
+                res = [exc] * len(items)
+                if len(items) > 1:
+                    for j, it in enumerate(items):
+                        try:
+                            res[j] = fn([it])[0]
+                        except Exception as exc1:
+                            res[j] = exc1
+            for (prob, _), r in zip(items, res):
+                out[prob] = r
+        for prob, r in out.items():
+            self.results[prob] = r
+            self.events.pop(prob).set()
+
+    # -- reporting -------------------------------------------------------------------------
+    def stats(self):
+        lat = np.array([r.latency() for r in self.finished if r.error is None])
+        return {"finished": len(self.finished), "failed": sum(r.error is not None for r in self.finished),
+                "rounds": self.rounds, "launch_groups": dict(self.launches),
+                "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
+                "max_batch": int(max(self.batch_sizes)) if self.batch_sizes else 0,
+                "max_active": self.max_active_seen,
+                "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+                "p99_s": float(np.percentile(lat, 99)) if lat.size else None}
+
+
+class ServingEngine(Scheduler):
+    """Continuous-batching matcher on the current CUDA device (default stream):
+    submit() from any thread, run() drives the GPU.  line_search_precision:
+    'fp32c' (default) or 'fp64' data-term values, see the module docstring."""
+
+    def __init__(self, hbm_budget_bytes=150e9, max_active=64, line_search_precision="fp32c"):
+        require_cuda()
+        _lib.load()
+        if line_search_precision not in ("fp32c", "fp64"):
+            raise ValueError("line_search_precision must be 'fp32c' or 'fp64'")
+        super().__init__(hbm_budget_bytes, max_active)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.lsp = line_search_precision
+
+    def _make_problem(self, req):
+        return _Problem(req, self)
+
+    # -- ragged operations -----------------------------------------------------------------
+    def _dataterm(self, probs, verts, grad, precision, target_self=False):
+        """Ragged data term (lddmm_ragged_dataterm_*): NormDef values, Norm0 of
+        the targets (target_self) or NormGradient w.r.t. the vertices."""
+        req0 = probs[0].req
+        k, d = req0.f0.shape[1], req0.v0.shape[1]
+        v_off, c_off, c2_off = [0], [0], [0]
+        cells, vptr, vidx, c2, s2 = [], [], [], [], []
+        for p, v in zip(probs, verts):
+            shp = p.tshape if target_self else p.dshape
+            nc = shp.cells.shape[0]
+            cells.append(shp.cells + v_off[-1])
+            vptr.append(shp.vptr[:-1] + c_off[-1] * k)
+            vidx.append(shp.vidx + c_off[-1] * k)
+            v_off.append(v_off[-1] + v.shape[0])
+            c_off.append(c_off[-1] + nc)
+            if target_self:
+                c2_off.append(0)
+            else:
+                c2.append(p.tc)
+                s2.append(p.tv)
+                c2_off.append(c2_off[-1] + p.tc.shape[0])
+        dev = self.device
+        V = torch.cat(verts)
+        C = torch.cat(cells)
+        VP = torch.cat(vptr + [torch.full((1,), c_off[-1] * k, dtype=torch.int64, device=dev)])
+        VI = torch.cat(vidx)
+        C2 = torch.cat(c2) if c2 else None
+        S2 = torch.cat(s2) if s2 else None
+        nreq = len(probs)
+        norm = NORMS[req0.param.errorType]
+        order = _order(req0.param.KparDist)
+        sfx = "f32c" if precision == "fp32c" else "f64"
+        energy = None if grad else torch.empty(nreq, dtype=torch.float64, device=dev)
+        px = torch.empty_like(V) if grad else None
+        vo, co, c2o = _i64(v_off), _i64(c_off), _i64(c2_off)
+        wsb = _lib.query("lddmm_ragged_dataterm_%s_workspace" % sfx, nreq, k, norm, vo, co, c2o, d, order,
+                         0 if grad else 1, 1 if grad else 0)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_ragged_dataterm_" + sfx, nreq, k, norm, vo, co, c2o, ptr(V), d, ptr(C),
+                  ptr(C2) if C2 is not None else None, ptr(S2) if S2 is not None else None,
+                  _f64([p.sigma_dist for p in probs]), order, 1e-10, 1e-10,
+                  ptr(energy) if energy is not None else None, ptr(VP), ptr(VI),
+                  ptr(px) if px is not None else None, ptr(ws), wsb, stream_handle())
+        if grad:
+            return [px[v_off[i]:v_off[i + 1]] for i in range(nreq)]
+        return energy
+
+    def _do_norm0(self, items):
+        probs = [p for p, _ in items]
+        e = self._dataterm(probs, [p.v1 for p in probs], False, self.lsp, target_self=True).cpu().numpy()
+        return [float(e[i]) / p.s2 for i, p in enumerate(probs)]
+
+    def _do_value(self, items):
+        """Shooting + deformation energy (lddmm_ragged_shoot_f32c), then the data
+        term at the end points: objectiveFunDef + dataTerm (surfaceMatching.py:187-231)."""
+        probs = [p for p, _ in items]
+        T, d = probs[0].T, probs[0].dim
+        v_off = [0]
+        for p in probs:
+            v_off.append(v_off[-1] + p.npt)
+        dev = self.device
+        X0 = torch.cat([p.x0 for p in probs])
+        AT = torch.cat([a.reshape(-1, d) for _, a in items])
+        XT = torch.empty(((T + 1) * v_off[-1], d), dtype=torch.float64, device=dev)
+        E = torch.empty(len(probs), dtype=torch.float64, device=dev)
+        vo = _i64(v_off)
+        order = _order(probs[0].req.param.KparDiff)
+        wsb = _lib.query("lddmm_ragged_shoot_f32c_workspace", len(probs), vo, d, T, order)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_ragged_shoot_f32c", len(probs), vo, d, ptr(X0), ptr(AT), T,
+                  _f64([p.sigma_def for p in probs]), order, _f64([p.req.regweight for p in probs]), ptr(XT),
+                  ptr(E), ptr(ws), wsb, stream_handle())
+        xts = [XT[(T + 1) * v_off[i]:(T + 1) * v_off[i + 1]].view(T + 1, p.npt, d) for i, p in enumerate(probs)]
+        D = self._dataterm(probs, [xt[-1] for xt in xts], False, self.lsp)
+        s2 = torch.tensor([p.s2 for p in probs], dtype=torch.float64, device=dev)
+        tot = (E + D / s2).cpu().numpy()
+        for p in probs:
+            p.calls["value"] += 1
+        return [(float(tot[i]), xts[i]) for i in range(len(probs))]
+
+    def _do_grad(self, items):
+        """grd.diff = (2 rw a - p_{t+1}) from the adjoint with p_T = -grad D / sigmaError^2
+        (surfaceMatching.py:301-327, pointEvolution.py:735-817)."""
+        probs = [p for p, _ in items]
+        T, d = probs[0].T, probs[0].dim
+        pxs = self._dataterm(probs, [p.xt[-1] for p in probs], True, "fp32c")
+        v_off = [0]
+        for p in probs:
+            v_off.append(v_off[-1] + p.npt)
+        XT = torch.cat([p.xt.reshape(-1, d) for p in probs])
+        AT = torch.cat([p.at.reshape(-1, d) for p in probs])
+        PX1 = torch.cat([px / (-p.s2) for p, px in zip(probs, pxs)])
+        PXT = torch.empty_like(XT)
+        DAT = torch.empty_like(AT)
+        vo = _i64(v_off)
+        order = _order(probs[0].req.param.KparDiff)
+        wsb = _lib.query("lddmm_ragged_covector_f32c_workspace", len(probs), vo, d, T, order)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_ragged_covector_f32c", len(probs), vo, d, ptr(XT), ptr(AT), T, ptr(PX1),
+                  _f64([p.sigma_def for p in probs]), order, _f64([p.req.regweight for p in probs]), ptr(PXT),
+                  ptr(DAT), ptr(ws), wsb, stream_handle())
+        for p in probs:
+            p.calls["grad"] += 1
+        return [DAT[T * v_off[i]:T * v_off[i + 1]].view(T, p.npt, d) for i, p in enumerate(probs)]
+
+    def _do_dot(self, items):
+        """sum_t <g2_t, K(x_t) g1_t> for every g2 (surfaceMatching.py:353-377):
+        one applyK segment per (request, t) in a single ragged launch."""
+        probs = [p for p, _ in items]
+        T, d = probs[0].T, probs[0].dim
+        XT = torch.cat([p.xt[:T].reshape(-1, d) for p in probs])
+        G1 = torch.cat([g1.reshape(-1, d) for _, (g1, _) in items])
+        starts, counts, sig = [], [], []
+        row = 0
+        for p in probs:
+            for t in range(T):
+                starts.append(row + t * p.npt)
+                counts.append(p.npt)
+                sig.append(p.sigma_def)
+            row += T * p.npt
+        U = torch.empty_like(XT)
+        st, cn = _i64(starts), _i64(counts)
+        order = _order(probs[0].req.param.KparDiff)
+        wsb = _lib.query("lddmm_ragged_applyk_f32c_workspace", len(starts), cn, cn, d, d, order)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_ragged_applyk_f32c", len(starts), st, cn, st, cn, d, ptr(XT), ptr(XT), ptr(G1), d,
+                  _f64(sig), order, ptr(U), ptr(ws), wsb, stream_handle())
+        outs = []
+        row = 0
+        for p, (_, g2s) in items:
+            u = U[row:row + T * p.npt].reshape(-1)
+            row += T * p.npt
+            G2 = torch.stack([g.reshape(-1) for g in g2s])
+            outs.append(G2 @ u)
+            p.calls["dot"] += 1
+        host = torch.cat(outs).cpu().numpy()
+        res, k = [], 0
+        for _, (_, g2s) in items:
+            res.append(host[k:k + len(g2s)].copy())
+            k += len(g2s)
+        return res
+
+def serve(requests, **engine_kw):
+    """Runs a list of requests (arrival times already set, or now) to completion."""
+    eng = ServingEngine(**engine_kw)
+    for r in requests:
+        eng.submit(r, arrival=r.arrival)
+    eng.run()
+    return eng

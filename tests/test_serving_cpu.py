@@ -1,0 +1,207 @@
+"""Host logic of the continuous-batching scheduler (no GPU): admission under
+the slot count and the HBM budget, late arrivals, grouping of work into one
+launch per kind, error isolation and result routing.  The work items are
+computed by a numpy stand-in engine (quadratic objectives), so every request's
+answer is known in closed form."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from registration_b200 import serving
+
+
+class _Dir:
+    def __init__(self, diff):
+        self.diff = diff
+
+
+class _ToyProblem:
+    """E(a) = sum w (a - c)^2 + 1; the cg protocol with every evaluation posted."""
+
+    def __init__(self, req, eng):
+        self.req, self.engine = req, eng
+        self.at = np.zeros(req.n)
+        self.atTry = self.at
+        self.xt = None
+        self.obj = self.objTry = None
+        self.gradCoeff = 1.0
+        self.iters = 0
+        self.converged = False
+        self.calls = {"value": 0, "grad": 0, "dot": 0}
+
+    def getVariable(self):
+        return [self.at]
+
+    def objectiveFun(self):
+        if self.obj is None:
+            self.obj = self.engine.post(self, "value", self.at)
+        return self.obj
+
+    def updateTry(self, dir, eps, objRef=None):
+        a = self.at - eps * dir.diff
+        e = self.engine.post(self, "value", a)
+        if objRef is None or e < objRef:
+            self.atTry, self.objTry = a, e
+        return e
+
+    def getGradient(self, coeff=1.0):
+        return _Dir(self.engine.post(self, "grad", self.at) / coeff)
+
+    def dotProduct(self, g1, g2):
+        return self.engine.post(self, "dot", (g1.diff, [g.diff for g in g2]))
+
+    def addProd(self, d1, d2, beta):
+        return _Dir(d1.diff + beta * d2.diff)
+
+    def copyDir(self, d0):
+        return _Dir(d0.diff.copy())
+
+    def acceptVarTry(self):
+        self.at, self.obj = self.atTry, self.objTry
+
+    def endOfIteration(self):
+        self.iters += 1
+
+
+class _ToyRequest:
+    def __init__(self, rid, n, group=0, fail=False, max_iter=30):
+        rng = np.random.default_rng(rid)
+        self.rid, self.n, self.group, self.fail = rid, n, group, fail
+        self.w = rng.uniform(0.5, 2.0, n)
+        self.c = rng.standard_normal(n)
+        self.max_iter = max_iter
+        self.arrival = self.start = self.finish = None
+        self.result = self.error = None
+        self.done = threading.Event()
+
+    def hbm_bytes(self):
+        return 1000 * self.n
+
+    def latency(self):
+        return self.finish - self.arrival
+
+
+class _ToyEngine(serving.Scheduler):
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        self.launch_log = []
+        self.lock = threading.Lock()
+
+    def _make_problem(self, req):
+        return _ToyProblem(req, self)
+
+    def _log(self, kind, items):
+        self.launch_log.append((kind, sorted(p.req.rid for p, _ in items), len({p.req.group for p, _ in items})))
+
+    def _do_value(self, items):
+        self._log("value", items)
+        out = []
+        for p, a in items:
+            if p.req.fail:
+                raise RuntimeError("planted failure")
+            out.append(float((p.req.w * (a - p.req.c) ** 2).sum() + 1.0))
+            p.calls["value"] += 1
+        return out
+
+    def _do_grad(self, items):
+        self._log("grad", items)
+        return [2 * p.req.w * (a - p.req.c) for p, a in items]
+
+    def _do_dot(self, items):
+        self._log("dot", items)
+        return [np.array([float((g1 * g).sum()) for g in g2s]) for p, (g1, g2s) in items]
+
+
+def _alone(req):
+    eng = _ToyEngine()
+    r = _ToyRequest(req.rid, req.n, req.group, req.fail, req.max_iter)
+    eng.submit(r)
+    eng.run()
+    return r
+
+
+def test_all_requests_finish_and_match_alone():
+    reqs = [_ToyRequest(i, 5 + 3 * i) for i in range(8)]
+    eng = _ToyEngine(max_active=8)
+    for r in reqs:
+        eng.submit(r)
+    eng.run()
+    st = eng.stats()
+    assert st["finished"] == 8 and st["failed"] == 0 and st["max_batch"] == 8
+    for r in reqs:
+        a = _alone(r)
+        assert r.result["obj"] == a.result["obj"] and np.array_equal(r.result["at"], a.result["at"])
+        # the minimiser of the quadratic is c, E = 1
+        assert abs(r.result["obj"] - 1.0) < 1e-6
+
+
+def test_slot_count_and_budget_limit_admission():
+    reqs = [_ToyRequest(i, 10) for i in range(6)]
+    eng = _ToyEngine(max_active=3)
+    for r in reqs:
+        eng.submit(r)
+    eng.run()
+    assert eng.stats()["max_active"] == 3
+    assert max(len(rids) for _, rids, _ in eng.launch_log) <= 3
+    reqs = [_ToyRequest(i, 10) for i in range(6)]
+    eng = _ToyEngine(hbm_budget_bytes=2 * 10 * 1000 + 1)     # two requests' state
+    for r in reqs:
+        eng.submit(r)
+    eng.run()
+    assert eng.stats()["max_active"] == 2 and eng.stats()["finished"] == 6
+
+
+def test_request_above_budget_is_rejected_others_served():
+    big, small = _ToyRequest(0, 100), _ToyRequest(1, 5)
+    eng = _ToyEngine(hbm_budget_bytes=50 * 1000)
+    eng.submit(big)
+    eng.submit(small)
+    eng.run()
+    assert isinstance(big.error, MemoryError) and small.error is None
+
+
+def test_late_arrivals_join_running_batches():
+    reqs = [_ToyRequest(i, 8, max_iter=200) for i in range(4)]
+    t0 = time.perf_counter()
+    eng = _ToyEngine()
+    for j, r in enumerate(reqs):
+        eng.submit(r, arrival=t0 + 0.02 * j)
+    eng.run()
+    for r in reqs:
+        assert r.start >= r.arrival and r.error is None
+        a = _alone(r)
+        assert r.result["obj"] == a.result["obj"]
+
+
+def test_groups_never_share_a_launch_and_failures_are_isolated():
+    reqs = [_ToyRequest(0, 6, group=0), _ToyRequest(1, 7, group=1), _ToyRequest(2, 8, group=0),
+            _ToyRequest(3, 9, group=1, fail=True)]
+    eng = _ToyEngine()
+    for r in reqs:
+        eng.submit(r)
+    eng.run()
+    assert all(ngroups == 1 for _, _, ngroups in eng.launch_log)
+    assert isinstance(reqs[3].error, RuntimeError)
+    for r in reqs[:3]:
+        assert r.error is None and r.result["obj"] == _alone(r).result["obj"]
+
+
+def test_latency_percentiles_reported():
+    reqs = [_ToyRequest(i, 4) for i in range(5)]
+    eng = _ToyEngine()
+    for r in reqs:
+        eng.submit(r)
+    eng.run()
+    st = eng.stats()
+    assert 0 < st["p50_s"] <= st["p99_s"]
+
+
+@pytest.mark.parametrize("bad", ["errorType"])
+def test_match_request_validation(bad):
+    class P:
+        timeStep = 0.1
+        errorType = "hausdorff"
+    with pytest.raises(ValueError):
+        serving.MatchRequest(None, None, P())
