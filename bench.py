@@ -267,9 +267,10 @@ def run_curve(args):
     import logging
     logging.disable(logging.INFO)
     iters = args.iters or 50
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.02
     v, vt = curve_problem()
-    config = {"workload": "curve matching: ellipse 256 vertices, gauss sigma 0.5, current sigma 0.5, sigmaError 1, "
-                          "T 10, %d cg iterations" % iters}
+    config = {"workload": "curve matching: ellipse 256 vertices, gauss sigma 0.5, current sigma 0.5, sigmaError %g, "
+                          "T 10, %d cg iterations" % (sig_err, iters)}
     if args.impl == "reference":
         import oracle
         from oracle import lddmm_ref as ref
@@ -278,7 +279,7 @@ def run_curve(args):
         times, objs = [], []
         for s_ in range(max(1, args.warmup) + args.steps):
             param = ref.MatchingParam(timeStep=0.1, KparDiff=ref.Kernel(name="gauss", sigma=0.5),
-                                      KparDist=ref.Kernel(name="gauss", sigma=0.5), sigmaError=1.0,
+                                      KparDist=ref.Kernel(name="gauss", sigma=0.5), sigmaError=sig_err,
                                       errorType="current", curves=True)
             cm = ref.CurveMatching(ref.Curve(pointSet=v), ref.Curve(pointSet=vt), param, maxIter=iters)
             t0 = time.perf_counter()
@@ -302,7 +303,7 @@ def run_curve(args):
     def match(precision):
         param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
                                       KparDist=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
-                                      sigmaError=1.0, errorType="current")
+                                      sigmaError=sig_err, errorType="current")
         cm = CM.CurveMatching(Template=cv.Curve(pointSet=v), Target=cv.Curve(pointSet=vt), param=param,
                               maxIter=iters, saveRate=0)
         torch.cuda.synchronize()
@@ -325,7 +326,7 @@ def run_curve(args):
         oracle.build()
         oracle.set_num_threads(os.cpu_count() or 1)
         param = ref.MatchingParam(timeStep=0.1, KparDiff=ref.Kernel(name="gauss", sigma=0.5),
-                                  KparDist=ref.Kernel(name="gauss", sigma=0.5), sigmaError=1.0, errorType="current",
+                                  KparDist=ref.Kernel(name="gauss", sigma=0.5), sigmaError=sig_err, errorType="current",
                                   curves=True)
         rcm = ref.CurveMatching(ref.Curve(pointSet=v), ref.Curve(pointSet=vt), param, maxIter=iters)
         t0 = time.perf_counter()
@@ -347,9 +348,10 @@ def run_surface(args):
     import logging
     logging.disable(logging.INFO)
     iters = args.iters or 100
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
     v, f, vt = surface_problem()
     config = {"workload": "surface matching: icosphere %d vertices / %d faces, 8 bumps, gauss sigma 0.2, varifold "
-                          "sigma 0.1, sigmaError 1, T 10, %d cg iterations" % (len(v), len(f), iters)}
+                          "sigma 0.1, sigmaError %g, T 10, %d cg iterations" % (len(v), len(f), sig_err, iters)}
     import torch
     from registration_b200 import kernelFunctions as kf
     from registration_b200 import surfaceMatching as SM
@@ -359,7 +361,7 @@ def run_surface(args):
         param = SM.SurfaceMatchingParam(timeStep=0.1,
                                         KparDiff=kf.Kernel(name="gauss", sigma=0.2, precision=precision),
                                         KparDist=kf.Kernel(name="gauss", sigma=0.1, precision=precision),
-                                        sigmaError=1.0, errorType="varifold")
+                                        sigmaError=sig_err, errorType="varifold")
         sm = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v]), Target=sf.Surface(FV=[f, vt]), param=param,
                                 maxIter=maxit, testGradient=False)
         torch.cuda.synchronize()
@@ -580,7 +582,7 @@ def run_serving(args):
     import torch
     from registration_b200 import serving
     iters = args.iters or 50
-    sig_err = args.sigma_error if args.sigma_error is not None else 0.1
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
     R = args.requests
     t_prep = time.perf_counter()
     stream = serving_stream(R, args.seed, iters, sig_err)
@@ -623,13 +625,15 @@ def run_serving(args):
     lat = np.array([r.latency() for r in ok])
     its = np.array([r.result["iters"] for r in ok])
     thr = len(ok) / span
-    # 3. one-at-a-time FP64 GPU solves of six requests across the size range
+    # 3. one-at-a-time solves of six requests across the size range: the plain
+    #    FP64 GPU driver (SurfaceMatching, FP64 kernels, FP64 line search), and
+    #    this engine serving one request alone (FP32c, no batching)
     from registration_b200 import kernelFunctions as kf
     from registration_b200 import surfaceMatching as SM
     from registration_b200 import surfaces as sf
     order = np.argsort(sizes)
     pick = [int(order[int(q * (R - 1))]) for q in (0.0, 0.2, 0.4, 0.6, 0.8, 1.0)]
-    base_it = 3
+    base_it = 4
     samples = []
     for idx in pick:
         r = stream[idx]
@@ -647,21 +651,40 @@ def run_serving(args):
             ta = time.perf_counter()
             sm.optimizeMatching()
             torch.cuda.synchronize()
-            return time.perf_counter() - ta, sm
+            return time.perf_counter() - ta, sm.iter
 
-        t1, sm1 = solve(1)
-        tk, smk = solve(base_it)
-        per_it = (tk - t1) / max(1, smk.iter - sm1.iter) if smk.iter > sm1.iter else tk / max(1, smk.iter)
-        samples.append({"V": int(r.n), "seconds_1_iter": t1, "seconds_%d_iter" % base_it: tk,
-                        "iters": int(smk.iter), "seconds_per_iter": per_it, "setup_seconds": max(0.0, t1 - per_it)})
+        def alone(maxit):
+            q = _fresh([r])[0]
+            q.max_iter = maxit
+            torch.cuda.synchronize()
+            ta = time.perf_counter()
+            serving.serve([q], max_active=1)
+            torch.cuda.synchronize()
+            return time.perf_counter() - ta, q.result["iters"]
+
+        def two_point(fn):
+            fn(1)   # warm-up: workspaces, first-touch
+            t1, i1 = fn(1)
+            tk, ik = fn(base_it)
+            per = (tk - t1) / (ik - i1) if ik > i1 else tk / max(1, ik)
+            return {"seconds_1": t1, "iters_1": int(i1), "seconds_k": tk, "iters_k": int(ik),
+                    "seconds_per_iter": per, "setup_seconds": max(0.0, t1 - i1 * per)}
+
+        samples.append({"V": int(r.n), "fp64_one_at_a_time": two_point(solve), "fp32c_alone": two_point(alone)})
     Vs = np.array([s_["V"] for s_ in samples], dtype=np.float64)
     A = np.stack([np.ones_like(Vs), Vs ** 2], axis=1)
-    coef_it, *_ = np.linalg.lstsq(A, np.array([s_["seconds_per_iter"] for s_ in samples]), rcond=None)
-    coef_set, *_ = np.linalg.lstsq(A, np.array([s_["setup_seconds"] for s_ in samples]), rcond=None)
     it_by_rid = {r.rid: r.result["iters"] for r in ok}
-    pred = sum(max(0.0, coef_set[0] + coef_set[1] * n ** 2)
-               + max(1, it_by_rid.get(r.rid, iters)) * max(0.0, coef_it[0] + coef_it[1] * n ** 2)
-               for r, n in zip(stream, sizes))
+
+    def stream_seconds(key):
+        c_it, *_ = np.linalg.lstsq(A, np.array([s_[key]["seconds_per_iter"] for s_ in samples]), rcond=None)
+        c_set, *_ = np.linalg.lstsq(A, np.array([s_[key]["setup_seconds"] for s_ in samples]), rcond=None)
+        tot = sum(max(0.0, c_set[0] + c_set[1] * n ** 2)
+                  + max(1, it_by_rid.get(r.rid, iters)) * max(0.0, c_it[0] + c_it[1] * n ** 2)
+                  for r, n in zip(stream, sizes))
+        return tot, [float(c_) for c_ in c_it], [float(c_) for c_ in c_set]
+
+    pred, coef_it, coef_set = stream_seconds("fp64_one_at_a_time")
+    pred32, coef_it32, coef_set32 = stream_seconds("fp32c_alone")
     base_thr = R / pred
     # CPU: the FP64 C/OpenMP oracle's per-call timings on the median request x its served call counts
     cpu = None
@@ -685,9 +708,10 @@ def run_serving(args):
            "converged": int(sum(r.result["converged"] for r in ok)),
            "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
            "one_at_a_time_fp64_gpu": {"matches_per_s": base_thr, "seconds_per_stream": pred,
-                                      "per_iter_fit_s": [float(c_) for c_ in coef_it],
-                                      "setup_fit_s": [float(c_) for c_ in coef_set], "samples": samples},
-           "speedup_vs_one_at_a_time_fp64": thr / base_thr, "prep_seconds": t_prep, "clocks": clk,
+                                      "per_iter_fit_s": coef_it, "setup_fit_s": coef_set},
+           "one_at_a_time_fp32c_engine": {"matches_per_s": R / pred32, "seconds_per_stream": pred32,
+                                          "per_iter_fit_s": coef_it32, "setup_fit_s": coef_set32},
+           "samples": samples, "speedup_vs_one_at_a_time_fp64": thr / base_thr, "prep_seconds": t_prep, "clocks": clk,
            "cpu_baseline": cpu,
            "e2e": {"value": thr, "unit": "matches/s", "h2d_bytes_per_step": h2d // max(1, len(ok)),
                    "d2h_bytes_per_step": d2h // max(1, len(ok))}})

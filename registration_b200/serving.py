@@ -225,6 +225,7 @@ class Scheduler:
         self.batch_sizes = []
         self.busy_seconds = 0.0
         self.max_active_seen = 0
+        self.peak_hbm = 0.0
 
     # -- request side ------------------------------------------------------------------
     def submit(self, req, arrival=None):
@@ -286,6 +287,7 @@ class Scheduler:
                 elif (len(self.active) + len(start) < self.max_active
                       and self.hbm_in_use + req.hbm_bytes() <= self.hbm_budget):
                     self.hbm_in_use += req.hbm_bytes()
+                    self.peak_hbm = max(self.peak_hbm, self.hbm_in_use)
                     start.append(req)
                 else:
                     keep.append(req)
@@ -374,7 +376,7 @@ class Scheduler:
                 "rounds": self.rounds, "launch_groups": dict(self.launches),
                 "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
                 "max_batch": int(max(self.batch_sizes)) if self.batch_sizes else 0,
-                "max_active": self.max_active_seen,
+                "max_active": self.max_active_seen, "peak_hbm_bytes": self.peak_hbm,
                 "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
                 "p99_s": float(np.percentile(lat, 99)) if lat.size else None}
 

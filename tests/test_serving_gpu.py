@@ -180,10 +180,9 @@ def test_ragged_shoot_alone_equals_mix(problems):
         pa, da = _ragged_cov(xa, [p["at"]], [p["px1"]], [p["sigma"]], [p["rw"]])
         assert torch.equal(pa[0], pxts[i]) and torch.equal(da[0], dats[i])
     # a different mix (reversed order, one request left out)
-    sub = problems[::-1][:3]
-    xs, Es = _ragged_shoot(*args(sub))
-    for j, p in enumerate(sub):
-        i = problems.index(p)
+    idx = [3, 2, 1]
+    xs, Es = _ragged_shoot(*args([problems[i] for i in idx]))
+    for j, i in enumerate(idx):
         assert torch.equal(xs[j], xts[i]) and float(Es[j]) == float(E[i])
 
 
@@ -278,14 +277,15 @@ def test_serving_late_arrivals_and_hbm_budget_are_bit_identical():
     late = _make_requests(range(4))
     t0 = time.perf_counter()
     for j, r in enumerate(late):
-        r.arrival = t0 + 0.05 * j
+        r.arrival = t0 + 0.002 * j
     eng = serving.serve(late)
-    # a budget that admits one request at a time
+    # a budget that holds the largest request and little else
     one = _make_requests(range(4))
     for r in one:
         r.arrival = None
-    eng1 = serving.serve(one, hbm_budget_bytes=max(r.hbm_bytes() for r in one) * 1.5)
-    assert eng1.stats()["max_active"] == 1
+    budget = max(r.hbm_bytes() for r in one) * 1.01
+    eng1 = serving.serve(one, hbm_budget_bytes=budget)
+    assert eng1.stats()["peak_hbm_bytes"] <= budget and eng1.stats()["max_active"] < 4
     for a, b, c in zip(base, late, one):
         assert _result(a)["obj"] == _result(b)["obj"] == _result(c)["obj"]
         assert torch.equal(_result(a)["at"], _result(b)["at"]) and torch.equal(_result(a)["at"], _result(c)["at"])
