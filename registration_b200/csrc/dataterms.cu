@@ -80,12 +80,12 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr int PP = PointPlanes<Real>::N;
     double* c1 = ws.take<double>((size_t)a.nc * a.d);
     double* s1 = ws.take<double>((size_t)a.nc * a.d);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     const int nb = (int)std::min<long long>(1024, (a.nc + kDtThreads - 1) / kDtThreads);
     if (!ws.measuring()) {
         cell_geometry_kernel<<<grid_for(a.nc), 256, 0, st>>>(a.ncorner, a.v, a.nv, a.d, a.cells, a.nc, c1, s1);
-        bbox_center_kernel<<<1, 256, 0, st>>>(c1, a.nc, a.c2, a.nc2, a.d, center);
+        launch_bbox_center(c1, a.nc, a.c2, a.nc2, a.d, center, st);
     }
     if (a.energy != nullptr) {
         double* part = nullptr;

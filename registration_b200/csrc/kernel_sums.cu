@@ -35,7 +35,7 @@ int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) 
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * DIMB);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     if (ws.measuring()) return LDDMM_OK;
     if (ws.overflow()) {
         set_error("workspace too small: need %zu bytes, got %zu", ws.off, ws.cap);
@@ -53,7 +53,7 @@ int applyk_group(const ApplyKArgs& a, int col0, Workspace& ws, cudaStream_t st) 
     g.nvals = std::min(DIMB, a.dimb - col0);
     for (int c = 0; c < g.nvals; ++c) g.off[c] = col0 + c;
     g.mult = 1.0;
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    launch_bbox_center(a.x, a.n, a.y, a.m, a.d, center, st);
     pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
                                                                   pl.n_tpad);
     if constexpr (sizeof(Real) == 4) {
@@ -180,7 +180,7 @@ int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
     float4* tgt = ws.take<float4>((size_t)NT * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * D);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     typename Op::Params P{};
@@ -200,7 +200,7 @@ int difft_impl(const DiffKTArgs& a, Workspace& ws, cudaStream_t st) {
         gu.off[w] = (long long)i * a.n * a.dimb + c;
         gv.off[w] = (long long)i * a.m * a.dimb + c;
     }
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    launch_bbox_center(a.x, a.n, a.y, a.m, a.d, center, st);
     pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
                                                                   pl.n_tpad);
     pack_values_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(gu, a.n, tgt, pl.n_tpad, pl.n_tpad,
@@ -307,7 +307,7 @@ int div_impl(const ApplyKArgs& a, Workspace& ws, cudaStream_t st) {
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma, /*exact_tables=*/true);
     // (the reference's applyDivergence runs on its dense numpy matrices, which
@@ -319,7 +319,7 @@ int div_impl(const ApplyKArgs& a, Workspace& ws, cudaStream_t st) {
     P.tgt_stride = pl.n_tpad;
     for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
     for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x, a.n, a.y, a.m, a.d, center);
+    launch_bbox_center(a.x, a.n, a.y, a.m, a.d, center, st);
     pack_points_kernel<Real><<<grid_for(pl.n_tpad), 256, 0, st>>>(a.x, a.n, a.d, ks.scale, center, tgt, pl.n_tpad,
                                                                   pl.n_tpad);
     pack_points_kernel<Real><<<grid_for(pl.m_pad), 256, 0, st>>>(a.y, a.m, a.d, ks.scale, center, src, pl.m_pad,

@@ -9,33 +9,94 @@ namespace lddmm {
 // Centre of the bounding box of x (n, d) and y (m, d): center[0..d).  The
 // kernels are translation invariant, and packing coordinates relative to this
 // centre halves the magnitude (and so the FP32 rounding error) of the packed
-// coordinates.  One block; min/max do not depend on the reduction order.
-static __global__ void bbox_center_kernel(const double* __restrict__ x, long long n, const double* __restrict__ y,
-                                          long long m, int d, double* __restrict__ center) {
-    __shared__ double lo[3][256], hi[3][256];
-    double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
-    for (long long i = threadIdx.x; i < n + m; i += blockDim.x) {
+// coordinates.
+//
+// Many blocks reduce min / max of order-preserving 64-bit keys of the
+// coordinates with atomicMin / atomicMax: min and max are exact, so the result
+// does not depend on the order of the blocks.  The centre buffer holds
+// kCenterWords doubles: the centre in [0, 4) and the six keys in [4, 10).
+constexpr int kCenterWords = 16;
+constexpr long long kKeyMax = 0x7FFFFFFFFFFFFFFFLL;
+constexpr long long kKeyMin = -kKeyMax - 1;
+
+// signed-integer order of the keys == numeric order of the doubles (no NaN)
+LDDMM_D long long bbox_key(double v) {
+    const long long b = __double_as_longlong(v);
+    return b >= 0 ? b : (b ^ kKeyMax);
+}
+
+LDDMM_D double bbox_val(long long k) { return __longlong_as_double(k >= 0 ? k : (k ^ kKeyMax)); }
+
+// warp + block reduction of per-thread key bounds, then one atomic per block
+// and component into keys[0..3) (min) and keys[3..6) (max)
+LDDMM_D void bbox_block_commit(long long (&l)[3], long long (&h)[3], long long* keys) {
+    __shared__ long long sl[3][32], sh[3][32];
+    for (int off = 16; off > 0; off >>= 1)
+        for (int j = 0; j < 3; ++j) {
+            l[j] = min(l[j], __shfl_down_sync(0xffffffffu, l[j], off));
+            h[j] = max(h[j], __shfl_down_sync(0xffffffffu, h[j], off));
+        }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+        for (int j = 0; j < 3; ++j) {
+            sl[j][warp] = l[j];
+            sh[j][warp] = h[j];
+        }
+    __syncthreads();
+    if (warp == 0) {
+        for (int j = 0; j < 3; ++j) {
+            l[j] = lane < nw ? sl[j][lane] : kKeyMax;
+            h[j] = lane < nw ? sh[j][lane] : kKeyMin;
+        }
+        for (int off = 16; off > 0; off >>= 1)
+            for (int j = 0; j < 3; ++j) {
+                l[j] = min(l[j], __shfl_down_sync(0xffffffffu, l[j], off));
+                h[j] = max(h[j], __shfl_down_sync(0xffffffffu, h[j], off));
+            }
+        if (lane == 0)
+            for (int j = 0; j < 3; ++j) {
+                if (l[j] != kKeyMax) atomicMin(keys + j, l[j]);
+                if (h[j] != kKeyMin) atomicMax(keys + 3 + j, h[j]);
+            }
+    }
+}
+
+static __global__ void bbox_init_kernel(long long* __restrict__ keys) {
+    if (threadIdx.x < 6) keys[threadIdx.x] = threadIdx.x < 3 ? kKeyMax : kKeyMin;
+}
+
+static __global__ void bbox_keys_kernel(const double* __restrict__ x, long long n, const double* __restrict__ y,
+                                        long long m, int d, long long* __restrict__ keys) {
+    long long l[3] = {kKeyMax, kKeyMax, kKeyMax}, h[3] = {kKeyMin, kKeyMin, kKeyMin};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n + m;
+         i += (long long)gridDim.x * blockDim.x) {
         const double* p = i < n ? x + i * d : y + (i - n) * d;
         for (int j = 0; j < d; ++j) {
-            l[j] = fmin(l[j], p[j]);
-            h[j] = fmax(h[j], p[j]);
+            const long long k = bbox_key(p[j]);
+            l[j] = min(l[j], k);
+            h[j] = max(h[j], k);
         }
     }
-    for (int j = 0; j < 3; ++j) {
-        lo[j][threadIdx.x] = l[j];
-        hi[j][threadIdx.x] = h[j];
+    bbox_block_commit(l, h, keys);
+}
+
+static __global__ void bbox_finish_kernel(const long long* __restrict__ keys, int d, int nonempty,
+                                          double* __restrict__ center) {
+    if (threadIdx.x < 3) {
+        const int j = threadIdx.x;
+        center[j] = (j < d && nonempty) ? 0.5 * (bbox_val(keys[j]) + bbox_val(keys[3 + j])) : 0.0;
     }
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s)
-            for (int j = 0; j < 3; ++j) {
-                lo[j][threadIdx.x] = fmin(lo[j][threadIdx.x], lo[j][threadIdx.x + s]);
-                hi[j][threadIdx.x] = fmax(hi[j][threadIdx.x], hi[j][threadIdx.x + s]);
-            }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int j = 0; j < 3; ++j) center[j] = j < d && n + m > 0 ? 0.5 * (lo[j][0] + hi[j][0]) : 0.0;
+}
+
+// center: kCenterWords doubles of device memory (see above)
+inline void launch_bbox_center(const double* x, long long n, const double* y, long long m, int d, double* center,
+                               cudaStream_t st) {
+    long long* keys = reinterpret_cast<long long*>(center + 4);
+    const long long tot = n + m;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>(148 * 4, (tot + 2047) / 2048));
+    bbox_init_kernel<<<1, 32, 0, st>>>(keys);
+    bbox_keys_kernel<<<blocks, 256, 0, st>>>(x, n, y, m, d, keys);
+    bbox_finish_kernel<<<1, 32, 0, st>>>(keys, d, tot > 0 ? 1 : 0, center);
 }
 
 // Points: value j of row i is (x[i*d + j] - center[j]) * scale (zero for j >= d or i >= n).

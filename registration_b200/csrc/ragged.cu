@@ -52,6 +52,8 @@ struct RagSeg {
     double center[3];
     double rw;
     double extra;        // dt, or sign of the target set, ...
+    long long bkey[6];   // bounding-box keys (min x y z, max x y z), see bbox_key
+    int bb0, nbb;        // first bounding-box block of this segment, block count
 };
 
 // Host-side plan of a ragged launch.
@@ -83,7 +85,7 @@ RagPlan<Op> rag_plan(const std::vector<long long>& n, const std::vector<long lon
         g.spad = pl.m_pad;
         g.part = p.parts;
         g.split = pl.split;
-        g.nb = (int)std::max<long long>(1, std::min<long long>(64, (n[s] + kRagThreads - 1) / kRagThreads));
+        g.nb = (int)std::max<long long>(1, std::min<long long>(1024, (n[s] + kRagThreads - 1) / kRagThreads));
         g.eoff = p.eparts;
         SegDesc& d = p.desc[s];
         d.tgt = g.tgt;
@@ -119,68 +121,65 @@ LDDMM_D double rag_block_sum(double v) {
     return r;
 }
 
-// centre of the bounding box of rows [row0, row0 + n) of x (and, if y, of
-// [m0, m0 + m) of y): one block per segment
-static __global__ void rag_bbox_kernel(RagSeg* segs, int nseg, const double* __restrict__ x,
-                                       const double* __restrict__ y, int d) {
-    const int s = blockIdx.x;
-    if (s >= nseg) return;
-    RagSeg& g = segs[s];
-    __shared__ double lo[3][kRagThreads], hi[3][kRagThreads];
-    double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
+// Centre of the bounding box of each segment's rows: rows [row0, row0 + n) of x
+// (x0 of a trajectory block when XT0: rows (T+1) row0 + i) and, if y, rows
+// [m0, m0 + m) of y.  nbb blocks per segment reduce order-preserving keys with
+// atomics into the segment's bkey (exact, order independent).
+template <bool XT0>
+static __global__ void rag_bbox_keys_kernel(RagSeg* segs, int nseg, const double* __restrict__ x,
+                                            const double* __restrict__ y, int d, int T) {
+    const int b = blockIdx.x;
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].bb0 <= b) lo = mid; else hi = mid - 1;
+    }
+    RagSeg& g = segs[lo];
+    const int lb = b - g.bb0;
+    const double* base = x + (XT0 ? (long long)(T + 1) * g.row0 : g.row0) * d;
     const long long tot = g.n + (y ? g.m : 0);
-    for (long long i = threadIdx.x; i < tot; i += blockDim.x) {
-        const double* p = i < g.n ? x + (g.row0 + i) * d : y + (g.m0 + i - g.n) * d;
+    long long l[3] = {kKeyMax, kKeyMax, kKeyMax}, h[3] = {kKeyMin, kKeyMin, kKeyMin};
+    for (long long i = (long long)lb * blockDim.x + threadIdx.x; i < tot; i += (long long)g.nbb * blockDim.x) {
+        const double* p = i < g.n ? base + i * d : y + (g.m0 + i - g.n) * d;
         for (int j = 0; j < d; ++j) {
-            l[j] = fmin(l[j], p[j]);
-            h[j] = fmax(h[j], p[j]);
+            const long long k = bbox_key(p[j]);
+            l[j] = min(l[j], k);
+            h[j] = max(h[j], k);
         }
     }
-    for (int j = 0; j < 3; ++j) {
-        lo[j][threadIdx.x] = l[j];
-        hi[j][threadIdx.x] = h[j];
-    }
-    __syncthreads();
-    for (int k = kRagThreads / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k)
-            for (int j = 0; j < 3; ++j) {
-                lo[j][threadIdx.x] = fmin(lo[j][threadIdx.x], lo[j][threadIdx.x + k]);
-                hi[j][threadIdx.x] = fmax(hi[j][threadIdx.x], hi[j][threadIdx.x + k]);
-            }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int j = 0; j < 3; ++j) g.center[j] = (j < d && tot > 0) ? 0.5 * (lo[j][0] + hi[j][0]) : 0.0;
+    bbox_block_commit(l, h, g.bkey);
 }
 
-// centre of each request's initial points: rows [(T+1)*row0, (T+1)*row0 + n) of xt
-static __global__ void rag_bbox_xt0_kernel(RagSeg* segs, int nseg, const double* __restrict__ xt, int T, int d) {
-    const int s = blockIdx.x;
+static __global__ void rag_bbox_finish_kernel(RagSeg* segs, int nseg, int d, int with_y) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nseg) return;
     RagSeg& g = segs[s];
-    __shared__ double lo[3][kRagThreads], hi[3][kRagThreads];
-    double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
-    const double* base = xt + (long long)(T + 1) * g.row0 * d;
-    for (long long i = threadIdx.x; i < g.n; i += blockDim.x)
-        for (int j = 0; j < d; ++j) {
-            l[j] = fmin(l[j], base[i * d + j]);
-            h[j] = fmax(h[j], base[i * d + j]);
+    const bool nonempty = g.n + (with_y ? g.m : 0) > 0;
+    for (int j = 0; j < 3; ++j)
+        g.center[j] = (j < d && nonempty) ? 0.5 * (bbox_val(g.bkey[j]) + bbox_val(g.bkey[3 + j])) : 0.0;
+}
+
+// host: block layout of the bounding-box launch, initial keys; returns the block count
+static int rag_bbox_prepare(std::vector<RagSeg>& segs, bool with_y) {
+    int b = 0;
+    for (RagSeg& g : segs) {
+        const long long tot = g.n + (with_y ? g.m : 0);
+        g.nbb = (int)std::max<long long>(1, std::min<long long>(256, (tot + 2047) / 2048));
+        g.bb0 = b;
+        b += g.nbb;
+        for (int j = 0; j < 3; ++j) {
+            g.bkey[j] = kKeyMax;
+            g.bkey[3 + j] = kKeyMin;
         }
-    for (int j = 0; j < 3; ++j) {
-        lo[j][threadIdx.x] = l[j];
-        hi[j][threadIdx.x] = h[j];
     }
-    __syncthreads();
-    for (int k = kRagThreads / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k)
-            for (int j = 0; j < 3; ++j) {
-                lo[j][threadIdx.x] = fmin(lo[j][threadIdx.x], lo[j][threadIdx.x + k]);
-                hi[j][threadIdx.x] = fmax(hi[j][threadIdx.x], hi[j][threadIdx.x + k]);
-            }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int j = 0; j < 3; ++j) g.center[j] = (j < d && g.n > 0) ? 0.5 * (lo[j][0] + hi[j][0]) : 0.0;
+    return b;
+}
+
+template <bool XT0>
+static void rag_bbox_launch(RagSeg* dsegs, int nseg, int nbb, const double* x, const double* y, int d, int T,
+                            cudaStream_t st) {
+    rag_bbox_keys_kernel<XT0><<<nbb, kRagThreads, 0, st>>>(dsegs, nseg, x, y, d, T);
+    rag_bbox_finish_kernel<<<(nseg + 127) / 128, 128, 0, st>>>(dsegs, nseg, d, y != nullptr ? 1 : 0);
 }
 
 LDDMM_D void put_dup(float4* planes, long long stride, long long i, const float* v, int NV) {
@@ -251,11 +250,16 @@ static __global__ void rag_shoot_combine_kernel(const RagSeg* __restrict__ segs,
         const double* x0 = xt + (((long long)(T + 1) * g.row0 + (long long)step * g.n + i) * d);
         double* x1 = xt + (((long long)(T + 1) * g.row0 + (long long)(step + 1) * g.n + i) * d);
         const double* a0 = at + (((long long)T * g.row0 + (long long)step * g.n + i) * d);
+        double v[D];
+        for (int j = 0; j < D; ++j) v[j] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < g.split; ++k) {
+            const double* pk = part + (g.part + (long long)k * g.n + i) * D;
+            for (int j = 0; j < D; ++j) v[j] += pk[j];
+        }
         for (int j = 0; j < d; ++j) {
-            double v = 0.0;
-            for (int k = 0; k < g.split; ++k) v += part[(g.part + (long long)k * g.n + i) * D + j];
-            e += a0[j] * v;
-            x1[j] = x0[j] + g.extra * v;
+            e += a0[j] * v[j];
+            x1[j] = x0[j] + g.extra * v[j];
         }
     }
     const double r = rag_block_sum(e);
@@ -302,6 +306,7 @@ int rag_shoot_impl(int nseg, const int64_t* v_off, int d, const double* x0, cons
         pl.segs[s].rw = rw[s];
         pl.segs[s].extra = 1.0 / T;
     }
+    const int nbb = rag_bbox_prepare(pl.segs, false);
     LDDMM_TRY(rag_copy_table(pl.segs.data(), sizeof(RagSeg) * nseg, dsegs, st));
     LDDMM_TRY(rag_copy_table(pl.desc.data(), sizeof(SegDesc) * nseg, ddesc, st));
     LDDMM_TRY(rag_copy_table(padoff.data(), sizeof(long long) * (nseg + 1), dpad, st));
@@ -310,8 +315,7 @@ int rag_shoot_impl(int nseg, const int64_t* v_off, int d, const double* x0, cons
     for (int s = 0; s < nseg; ++s)
         LDDMM_TRY(cuda_check(cudaMemcpyAsync(xt + (T + 1) * v_off[s] * d, x0 + v_off[s] * d, sizeof(double) * n[s] * d,
                                              cudaMemcpyDeviceToDevice, st), "ragged shoot copy"));
-    rag_bbox_kernel<<<nseg, kRagThreads, 0, st>>>(dsegs, nseg, x0, nullptr, d);
-    // the bbox kernel reads x0 rows [row0, row0+n): row0 is the point offset of the request
+    rag_bbox_launch<false>(dsegs, nseg, nbb, x0, nullptr, d, 0, st);   // x0 rows [row0, row0 + n)
     KernelParams2 P{};
     P.src4 = src;
     P.src_stride = pl.ss;
@@ -386,10 +390,15 @@ static __global__ void rag_cov_combine_kernel(const RagSeg* __restrict__ segs, c
         double* pc = pxt + (((long long)(T + 1) * g.row0 + (long long)step * g.n + i) * d);
         const double* a = at + (((long long)T * g.row0 + (long long)step * g.n + i) * d);
         double* da = dat ? dat + (((long long)T * g.row0 + (long long)step * g.n + i) * d) : nullptr;
+        double f[D];
+        for (int j = 0; j < D; ++j) f[j] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < g.split; ++k) {
+            const double* pk = part + (g.part + (long long)k * g.n + i) * D;
+            for (int j = 0; j < D; ++j) f[j] += pk[j];
+        }
         for (int j = 0; j < d; ++j) {
-            double f = 0.0;
-            for (int k = 0; k < g.split; ++k) f += part[(g.part + (long long)k * g.n + i) * D + j];
-            pc[j] = pn[j] + g.extra * (g.dscale * f);
+            pc[j] = pn[j] + g.extra * (g.dscale * f[j]);
             if (da) da[j] = 2.0 * g.rw * a[j] - pn[j];
         }
     }
@@ -425,6 +434,7 @@ int rag_cov_impl(int nseg, const int64_t* v_off, int d, const double* xt, const 
         pl.segs[s].rw = rw[s];
         pl.segs[s].extra = 1.0 / T;
     }
+    const int nbb = rag_bbox_prepare(pl.segs, false);
     LDDMM_TRY(rag_copy_table(pl.segs.data(), sizeof(RagSeg) * nseg, dsegs, st));
     LDDMM_TRY(rag_copy_table(pl.desc.data(), sizeof(SegDesc) * nseg, ddesc, st));
     LDDMM_TRY(rag_copy_table(padoff.data(), sizeof(long long) * (nseg + 1), dpad, st));
@@ -432,7 +442,7 @@ int rag_cov_impl(int nseg, const int64_t* v_off, int d, const double* xt, const 
     for (int s = 0; s < nseg; ++s)
         LDDMM_TRY(cuda_check(cudaMemcpyAsync(pxt + ((T + 1) * v_off[s] + (long long)T * n[s]) * d, px1 + v_off[s] * d,
                                              sizeof(double) * n[s] * d, cudaMemcpyDeviceToDevice, st), "cov copy"));
-    rag_bbox_xt0_kernel<<<nseg, kRagThreads, 0, st>>>(dsegs, nseg, xt, T, d);
+    rag_bbox_launch<true>(dsegs, nseg, nbb, xt, nullptr, d, T, st);   // x_0 of each trajectory block
     KernelParams2 P{};
     P.src4 = src;
     P.src_stride = pl.ss;
@@ -497,11 +507,14 @@ static __global__ void rag_applyk_combine_kernel(const RagSeg* __restrict__ segs
         const int s = seg_lookup(rowoff, nseg, q);
         const RagSeg& g = segs[s];
         const long long i = q - rowoff[s];
-        for (int c = 0; c < dimb && c < DIMB; ++c) {
-            double v = 0.0;
-            for (int k = 0; k < g.split; ++k) v += part[(g.part + (long long)k * g.n + i) * DIMB + c];
-            f[q * dimb + c] = v;
+        double v[DIMB];
+        for (int c = 0; c < DIMB; ++c) v[c] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < g.split; ++k) {
+            const double* pk = part + (g.part + (long long)k * g.n + i) * DIMB;
+            for (int c = 0; c < DIMB; ++c) v[c] += pk[c];
         }
+        for (int c = 0; c < dimb && c < DIMB; ++c) f[q * dimb + c] = v[c];
     }
 }
 
@@ -536,11 +549,12 @@ int rag_applyk_impl(int nseg, const int64_t* t_start, const int64_t* t_count, co
         pl.segs[s].scale = ks.scale;
         pl.segs[s].dscale = ks.dscale;
     }
+    const int nbb = rag_bbox_prepare(pl.segs, true);
     LDDMM_TRY(rag_copy_table(pl.segs.data(), sizeof(RagSeg) * nseg, dsegs, st));
     LDDMM_TRY(rag_copy_table(pl.desc.data(), sizeof(SegDesc) * nseg, ddesc, st));
     LDDMM_TRY(rag_copy_table(padoff.data(), sizeof(long long) * (nseg + 1), dpad, st));
     LDDMM_TRY(rag_copy_table(rowoff.data(), sizeof(long long) * (nseg + 1), drow, st));
-    rag_bbox_kernel<<<nseg, kRagThreads, 0, st>>>(dsegs, nseg, x, y, d);
+    rag_bbox_launch<false>(dsegs, nseg, nbb, x, y, d, 0, st);
     KernelParams2 P{};
     P.src4 = src;
     P.src_stride = pl.ss;
@@ -605,8 +619,11 @@ static __global__ void rag_dt_value_kernel(const RagSeg* __restrict__ segs, int 
     double e = 0.0;
     for (long long i = (long long)lb * blockDim.x + threadIdx.x; i < g.n; i += (long long)g.nb * blockDim.x) {
         double z[4] = {0, 0, 0, 0};
-        for (int c = 0; c < nout; ++c)
-            for (int k = 0; k < g.split; ++k) z[c] += part[(g.part + (long long)k * g.n + i) * nout + c];
+#pragma unroll 4
+        for (int k = 0; k < g.split; ++k) {
+            const double* pk = part + (g.part + (long long)k * g.n + i) * nout;
+            for (int c = 0; c < nout && c < 4; ++c) z[c] += pk[c];
+        }
         const double* sv = s1 + (g.row0 + i) * d;
         if (norm == NCURRENT) {
             for (int j = 0; j < d; ++j) e += sv[j] * z[j];
@@ -629,8 +646,11 @@ static __global__ void rag_dt_grad_kernel(const RagSeg* __restrict__ segs, const
         const RagSeg& g = segs[sg];
         const long long i = q - rowoff[sg];
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int c = 0; c < nout; ++c)
-            for (int k = 0; k < g.split; ++k) acc[c] += part[(g.part + (long long)k * g.n + i) * nout + c];
+#pragma unroll 2
+        for (int k = 0; k < g.split; ++k) {
+            const double* pk = part + (g.part + (long long)k * g.n + i) * nout;
+            for (int c = 0; c < nout && c < 8; ++c) acc[c] += pk[c];
+        }
         const long long r = g.row0 + i;
         dt_grad_row(norm, acc, s1 + r * d, d, eps1, fac * g.dscale, z1 + r * d, dz1 + r * d);
     }
@@ -687,11 +707,12 @@ int rag_dt_sweep(const RagDataArgs& a, int kind, int grad, double sign2, const d
         pl.segs[s].scale = ks.scale;
         pl.segs[s].dscale = ks.dscale;
     }
+    const int nbb = rag_bbox_prepare(pl.segs, a.c2 != nullptr);
     LDDMM_TRY(rag_copy_table(pl.segs.data(), sizeof(RagSeg) * nseg, dsegs, st));
     LDDMM_TRY(rag_copy_table(pl.desc.data(), sizeof(SegDesc) * nseg, ddesc, st));
     LDDMM_TRY(rag_copy_table(padoff.data(), sizeof(long long) * (nseg + 1), dpad, st));
     LDDMM_TRY(rag_copy_table(rowoff.data(), sizeof(long long) * (nseg + 1), drow, st));
-    rag_bbox_kernel<<<nseg, kRagThreads, 0, st>>>(dsegs, nseg, c1, a.c2, a.d);
+    rag_bbox_launch<false>(dsegs, nseg, nbb, c1, a.c2, a.d, 0, st);
     typename Op::Params P{};
     P.src4 = src;
     P.src_stride = pl.ss;

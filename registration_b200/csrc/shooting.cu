@@ -197,7 +197,7 @@ int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     double* part = ws.take<double>((size_t)pl.split * a.n * D);
     const int nb = combine_blocks(a.n);
     double* epart = ws.take<double>((size_t)a.T * nb);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     typename Op::Params P{};
@@ -208,7 +208,7 @@ int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     set_poly(P, ks);
     const long long N = a.n * a.d;
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.xt, a.x0, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "shoot copy"));
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x0, a.n, nullptr, 0, a.d, center);
+    launch_bbox_center(a.x0, a.n, nullptr, 0, a.d, center, st);
     shoot_pack_kernel<Real, DUP><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.x0, a.at, a.n, a.d, ks.scale, center, tgt, pl.n_tpad, src, pl.m_pad, Op::PP, D, Op::NS);
     const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
@@ -328,7 +328,7 @@ int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     float4* tgt = ws.take<float4>((size_t)NT * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * D);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     typename Op::Params P{};
@@ -342,7 +342,7 @@ int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.pxt + (long long)a.T * N, a.px1, sizeof(double) * N,
                                          cudaMemcpyDeviceToDevice, st), "covector copy"));
     const int T = a.T;
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.xt, a.n, nullptr, 0, a.d, center);
+    launch_bbox_center(a.xt, a.n, nullptr, 0, a.d, center, st);
     cov_pack_kernel<Real, DUP><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.xt + (long long)(T - 1) * N, a.at + (long long)(T - 1) * N, a.px1, a.n, a.d, ks.scale, center, a.rw,
         tgt, pl.n_tpad, src, pl.m_pad, Op::PP, NT, Op::NS, W);
@@ -477,7 +477,7 @@ int epd_impl(const EPDArgs& a, Workspace& ws, cudaStream_t st) {
     float4* tgt = ws.take<float4>((size_t)Op::NS * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     double* part = ws.take<double>((size_t)pl.split * a.n * Op::NOUT);
-    double* center = ws.take<double>(4);
+    double* center = ws.take<double>(kCenterWords);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     typename Op::Params P{};
@@ -492,7 +492,7 @@ int epd_impl(const EPDArgs& a, Workspace& ws, cudaStream_t st) {
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.xt, a.x0, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "epdiff"));
     LDDMM_TRY(cuda_check(cudaMemcpyAsync(a.at, a.a0, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "epdiff"));
     const int nb = combine_blocks(a.n);
-    bbox_center_kernel<<<1, 256, 0, st>>>(a.x0, a.n, nullptr, 0, a.d, center);
+    launch_bbox_center(a.x0, a.n, nullptr, 0, a.d, center, st);
     for (int t = 0; t < a.T; ++t) {
         epd_pack_kernel<Real><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
             a.xt + t * N, a.at + t * N, a.n, a.d, ks.scale, center, tgt, pl.n_tpad, src, pl.m_pad, Op::PP, D,

@@ -226,6 +226,7 @@ class Scheduler:
         self.busy_seconds = 0.0
         self.max_active_seen = 0
         self.peak_hbm = 0.0
+        self.threads = []
 
     # -- request side ------------------------------------------------------------------
     def submit(self, req, arrival=None):
@@ -307,7 +308,9 @@ class Scheduler:
             with self.cv:
                 self.active.add(prob)
                 self.max_active_seen = max(self.max_active_seen, len(self.active))
-            threading.Thread(target=self._run_request, args=(prob,), daemon=True).start()
+            th = threading.Thread(target=self._run_request, args=(prob,), daemon=True)
+            self.threads.append(th)
+            th.start()
 
     def _can_admit(self, now):
         if not self.queue or self.queue[0].arrival > now:
@@ -322,7 +325,7 @@ class Scheduler:
             self._admit(time.perf_counter())
             with self.cv:
                 if not self.active and not self.queue:
-                    return
+                    break
                 ready = None
                 while True:
                     if self.active and len(self.pending) == len(self.active):
@@ -342,6 +345,10 @@ class Scheduler:
                 self._execute(ready)
                 self.busy_seconds += time.perf_counter() - t0
                 self.rounds += 1
+        # every request thread has finished its work; let them exit
+        for th in self.threads:
+            th.join()
+        self.threads = []
 
     def _execute(self, ready):
         groups = {}
