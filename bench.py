@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=512, help="requests of the serving stream")
     ap.add_argument("--sigma-error", type=float, default=None, help="sigmaError of the matching workloads")
     ap.add_argument("--max-active", type=int, default=64, help="serving slots")
+    ap.add_argument("--lanes", default="5000,16000",
+                    help="serving size-class bounds (vertex counts), comma separated, or 'none'")
     return ap.parse_args()
 
 
@@ -584,6 +586,8 @@ def run_serving(args):
     iters = args.iters or 50
     sig_err = args.sigma_error if args.sigma_error is not None else 0.01
     R = args.requests
+    lanes = () if args.lanes in ("", "none") else tuple(int(b) for b in args.lanes.split(","))
+    ekw = {"max_active": args.max_active, "lanes": lanes}
     t_prep = time.perf_counter()
     stream = serving_stream(R, args.seed, iters, sig_err)
     t_prep = time.perf_counter() - t_prep
@@ -591,18 +595,18 @@ def run_serving(args):
     config = {"workload": "served surface matching: %d requests, V ~ logU[2000, 50000] icosphere-derived, 4-16 "
                           "bumps, gauss sigma ~ U[0.05, 0.3], varifold sigma = sigma/2, sigmaError %g, T 10, %d cg "
                           "iterations max, Poisson arrivals at 80%% of measured capacity, %d slots, 150 GB HBM "
-                          "budget" % (R, sig_err, iters, args.max_active)}
+                          "budget, size lanes %s" % (R, sig_err, iters, args.max_active, list(lanes))}
     # warm-up: library load, workspace growth, cuBLAS handles
     warm = _fresh([stream[int(np.argmin(sizes))]])
     for r in warm:
         r.max_iter = 2
-    serving.serve(warm, max_active=args.max_active)
+    serving.serve(warm, **ekw)
     torch.cuda.synchronize()
     # 1. capacity, closed loop
     ncal = min(64, R)
     cal = _fresh(stream[:ncal])
     t0 = time.perf_counter()
-    serving.serve(cal, max_active=args.max_active)
+    serving.serve(cal, **ekw)
     torch.cuda.synchronize()
     cap = ncal / (time.perf_counter() - t0)
     # 2. open loop at 80% of capacity
@@ -615,7 +619,7 @@ def run_serving(args):
     arr = t_start + np.cumsum(gaps) - gaps[0]
     for r, a in zip(reqs, arr):
         r.arrival = float(a)
-    eng = serving.serve(reqs, max_active=args.max_active)
+    eng = serving.serve(reqs, **ekw)
     torch.cuda.synchronize()
     t_end = max(r.finish for r in reqs)
     clk = clocks.stop()
@@ -625,67 +629,71 @@ def run_serving(args):
     lat = np.array([r.latency() for r in ok])
     its = np.array([r.result["iters"] for r in ok])
     thr = len(ok) / span
-    # 3. one-at-a-time solves of six requests across the size range: the plain
-    #    FP64 GPU driver (SurfaceMatching, FP64 kernels, FP64 line search), and
-    #    this engine serving one request alone (FP32c, no batching)
-    from registration_b200 import kernelFunctions as kf
-    from registration_b200 import surfaceMatching as SM
-    from registration_b200 import surfaces as sf
-    order = np.argsort(sizes)
-    pick = [int(order[int(q * (R - 1))]) for q in (0.0, 0.2, 0.4, 0.6, 0.8, 1.0)]
-    base_it = 4
+    pred = pred32 = base_thr = None
+    coef_it = coef_set = coef_it32 = coef_set32 = None
     samples = []
-    for idx in pick:
-        r = stream[idx]
-        p = r.param
+    order = np.argsort(sizes)
+    if not args.no_fp64:
+        # 3. one-at-a-time solves of six requests across the size range: the plain
+        #    FP64 GPU driver (SurfaceMatching, FP64 kernels, FP64 line search), and
+        #    this engine serving one request alone (FP32c, no batching)
+        from registration_b200 import kernelFunctions as kf
+        from registration_b200 import surfaceMatching as SM
+        from registration_b200 import surfaces as sf
+        pick = [int(order[int(q * (R - 1))]) for q in (0.0, 0.2, 0.4, 0.6, 0.8, 1.0)]
+        base_it = 4
+        samples = []
+        for idx in pick:
+            r = stream[idx]
+            p = r.param
 
-        def solve(maxit):
-            param = SM.SurfaceMatchingParam(
-                timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=p.KparDiff.sigma, precision="fp64"),
-                KparDist=kf.Kernel(name="gauss", sigma=p.KparDist.sigma, precision="fp64"),
-                sigmaError=p.sigmaError, errorType="varifold")
-            sm = SM.SurfaceMatching(Template=sf.Surface(FV=[r.f0, r.v0]), Target=sf.Surface(FV=[r.f1, r.v1]),
-                                    param=param, maxIter=maxit, testGradient=False, verb=False,
-                                    lineSearchPrecision="fp64")
-            torch.cuda.synchronize()
-            ta = time.perf_counter()
-            sm.optimizeMatching()
-            torch.cuda.synchronize()
-            return time.perf_counter() - ta, sm.iter
+            def solve(maxit):
+                param = SM.SurfaceMatchingParam(
+                    timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=p.KparDiff.sigma, precision="fp64"),
+                    KparDist=kf.Kernel(name="gauss", sigma=p.KparDist.sigma, precision="fp64"),
+                    sigmaError=p.sigmaError, errorType="varifold")
+                sm = SM.SurfaceMatching(Template=sf.Surface(FV=[r.f0, r.v0]), Target=sf.Surface(FV=[r.f1, r.v1]),
+                                        param=param, maxIter=maxit, testGradient=False, verb=False,
+                                        lineSearchPrecision="fp64")
+                torch.cuda.synchronize()
+                ta = time.perf_counter()
+                sm.optimizeMatching()
+                torch.cuda.synchronize()
+                return time.perf_counter() - ta, sm.iter
 
-        def alone(maxit):
-            q = _fresh([r])[0]
-            q.max_iter = maxit
-            torch.cuda.synchronize()
-            ta = time.perf_counter()
-            serving.serve([q], max_active=1)
-            torch.cuda.synchronize()
-            return time.perf_counter() - ta, q.result["iters"]
+            def alone(maxit):
+                q = _fresh([r])[0]
+                q.max_iter = maxit
+                torch.cuda.synchronize()
+                ta = time.perf_counter()
+                serving.serve([q], max_active=1)
+                torch.cuda.synchronize()
+                return time.perf_counter() - ta, q.result["iters"]
 
-        def two_point(fn):
-            fn(1)   # warm-up: workspaces, first-touch
-            t1, i1 = fn(1)
-            tk, ik = fn(base_it)
-            per = (tk - t1) / (ik - i1) if ik > i1 else tk / max(1, ik)
-            return {"seconds_1": t1, "iters_1": int(i1), "seconds_k": tk, "iters_k": int(ik),
-                    "seconds_per_iter": per, "setup_seconds": max(0.0, t1 - i1 * per)}
+            def two_point(fn):
+                fn(1)   # warm-up: workspaces, first-touch
+                t1, i1 = fn(1)
+                tk, ik = fn(base_it)
+                per = (tk - t1) / (ik - i1) if ik > i1 else tk / max(1, ik)
+                return {"seconds_1": t1, "iters_1": int(i1), "seconds_k": tk, "iters_k": int(ik),
+                        "seconds_per_iter": per, "setup_seconds": max(0.0, t1 - i1 * per)}
 
-        samples.append({"V": int(r.n), "fp64_one_at_a_time": two_point(solve), "fp32c_alone": two_point(alone)})
-    Vs = np.array([s_["V"] for s_ in samples], dtype=np.float64)
-    A = np.stack([np.ones_like(Vs), Vs ** 2], axis=1)
-    it_by_rid = {r.rid: r.result["iters"] for r in ok}
+            samples.append({"V": int(r.n), "fp64_one_at_a_time": two_point(solve), "fp32c_alone": two_point(alone)})
+        Vs = np.array([s_["V"] for s_ in samples], dtype=np.float64)
+        A = np.stack([np.ones_like(Vs), Vs ** 2], axis=1)
+        it_by_rid = {r.rid: r.result["iters"] for r in ok}
 
-    def stream_seconds(key):
-        c_it, *_ = np.linalg.lstsq(A, np.array([s_[key]["seconds_per_iter"] for s_ in samples]), rcond=None)
-        c_set, *_ = np.linalg.lstsq(A, np.array([s_[key]["setup_seconds"] for s_ in samples]), rcond=None)
-        tot = sum(max(0.0, c_set[0] + c_set[1] * n ** 2)
-                  + max(1, it_by_rid.get(r.rid, iters)) * max(0.0, c_it[0] + c_it[1] * n ** 2)
-                  for r, n in zip(stream, sizes))
-        return tot, [float(c_) for c_ in c_it], [float(c_) for c_ in c_set]
+        def stream_seconds(key):
+            c_it, *_ = np.linalg.lstsq(A, np.array([s_[key]["seconds_per_iter"] for s_ in samples]), rcond=None)
+            c_set, *_ = np.linalg.lstsq(A, np.array([s_[key]["setup_seconds"] for s_ in samples]), rcond=None)
+            tot = sum(max(0.0, c_set[0] + c_set[1] * n ** 2)
+                      + max(1, it_by_rid.get(r.rid, iters)) * max(0.0, c_it[0] + c_it[1] * n ** 2)
+                      for r, n in zip(stream, sizes))
+            return tot, [float(c_) for c_ in c_it], [float(c_) for c_ in c_set]
 
-    pred, coef_it, coef_set = stream_seconds("fp64_one_at_a_time")
-    pred32, coef_it32, coef_set32 = stream_seconds("fp32c_alone")
-    base_thr = R / pred
+        pred, coef_it, coef_set = stream_seconds("fp64_one_at_a_time")
+        pred32, coef_it32, coef_set32 = stream_seconds("fp32c_alone")
+        base_thr = R / pred
     # CPU: the FP64 C/OpenMP oracle's per-call timings on the median request x its served call counts
     cpu = None
     if not args.no_cpu_baseline:
@@ -704,14 +712,16 @@ def run_serving(args):
            "p99_ms": 1e3 * float(np.percentile(lat, 99)), "capacity_closed_loop": cap,
            "offered_rate": 0.8 * cap, "span_s": span, "failed": st["failed"], "rounds": st["rounds"],
            "mean_batch": st["mean_batch"], "max_batch": st["max_batch"], "max_active": st["max_active"],
+           "lane_rounds": st["lane_rounds"],
            "iterations_mean": float(its.mean()), "iterations_min": int(its.min()),
            "converged": int(sum(r.result["converged"] for r in ok)),
            "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
            "one_at_a_time_fp64_gpu": {"matches_per_s": base_thr, "seconds_per_stream": pred,
                                       "per_iter_fit_s": coef_it, "setup_fit_s": coef_set},
-           "one_at_a_time_fp32c_engine": {"matches_per_s": R / pred32, "seconds_per_stream": pred32,
+           "one_at_a_time_fp32c_engine": {"matches_per_s": R / pred32 if pred32 else None,
+                                          "seconds_per_stream": pred32,
                                           "per_iter_fit_s": coef_it32, "setup_fit_s": coef_set32},
-           "samples": samples, "speedup_vs_one_at_a_time_fp64": thr / base_thr, "prep_seconds": t_prep, "clocks": clk,
+           "samples": samples, "speedup_vs_one_at_a_time_fp64": thr / base_thr if base_thr else None, "prep_seconds": t_prep, "clocks": clk,
            "cpu_baseline": cpu,
            "e2e": {"value": thr, "unit": "matches/s", "h2d_bytes_per_step": h2d // max(1, len(ok)),
                    "d2h_bytes_per_step": d2h // max(1, len(ok))}})

@@ -200,26 +200,48 @@ class _Problem:
         self.iters += 1
 
 
+class _Lane:
+    """One size class of requests: its own round loop (thread) and, on the GPU,
+    its own CUDA stream (smaller requests: higher stream priority)."""
+
+    def __init__(self, idx, bound):
+        self.idx = idx
+        self.bound = bound
+        self.active = set()
+        self.pending = {}        # problem -> (kind, payload)
+        self.rounds = 0
+        self.stream = None
+        self.thread = None
+
+
 class Scheduler:
-    """Admission, rounds and grouping of the continuous-batching loop.
+    """Admission, lanes, rounds and grouping of the continuous-batching loop.
 
     Subclasses provide _make_problem(req) and one _do_<kind>(items) method per
     kind of work ("norm0", "value", "grad", "dot"), each mapping a list of
-    (problem, payload) to a list of results (one launch per call).
-    hbm_budget_bytes: admission limit on the sum of the active requests'
-    resident state (MatchRequest.hbm_bytes); max_active: slot count."""
+    (problem, payload) to a list of results (one launch per call), and may
+    override _lane_context(lane) (the context a lane's work runs in).
 
-    def __init__(self, hbm_budget_bytes=150e9, max_active=64):
+    hbm_budget_bytes: admission limit on the sum of the active requests'
+    resident state (MatchRequest.hbm_bytes); max_active: slot count;
+    lanes: increasing request-size bounds (vertex counts) of the size classes,
+    the last one unbounded, e.g. (5000, 16000) -> three lanes.  Each lane waits
+    for its own requests only, so small requests are not held back by the
+    rounds of large ones."""
+
+    def __init__(self, hbm_budget_bytes=150e9, max_active=64, lanes=()):
         self.hbm_budget = float(hbm_budget_bytes)
         self.max_active = int(max_active)
+        bounds = sorted(float(b) for b in lanes) + [float("inf")]
+        self.lanes = [_Lane(k, b) for k, b in enumerate(bounds)]
         self.cv = threading.Condition()
+        self.stats_lock = threading.Lock()
         self.queue = []          # submitted, not admitted (sorted by arrival)
-        self.active = set()
-        self.pending = {}        # problem -> (kind, payload)
         self.results = {}
         self.events = {}
         self.finished = []
         self.hbm_in_use = 0.0
+        self.n_active = 0
         self.rounds = 0
         self.launches = {"norm0": 0, "value": 0, "grad": 0, "dot": 0}
         self.batch_sizes = []
@@ -227,6 +249,14 @@ class Scheduler:
         self.max_active_seen = 0
         self.peak_hbm = 0.0
         self.threads = []
+        self._stop = False
+
+    def _lane_of(self, req):
+        return next(l for l in self.lanes if req.n <= l.bound)
+
+    def _lane_context(self, lane):
+        import contextlib
+        return contextlib.nullcontext()
 
     # -- request side ------------------------------------------------------------------
     def submit(self, req, arrival=None):
@@ -242,7 +272,7 @@ class Scheduler:
         ev = threading.Event()
         with self.cv:
             self.events[prob] = ev
-            self.pending[prob] = (kind, payload)
+            prob.lane.pending[prob] = (kind, payload)
             self.cv.notify_all()
         ev.wait()
         res = self.results.pop(prob)
@@ -250,28 +280,44 @@ class Scheduler:
             raise res
         return res
 
-    def _run_request(self, prob):
-        req = prob.req
+    def _run_request(self, req, lane, slot):
+        """Request thread: builds the problem in its lane's context and runs the
+        optimiser.  `slot` is the placeholder counted active until the problem
+        exists."""
+        prob = None
         try:
-            # SurfaceMatching.optimizeMatching (surfaceMatching.py:474-484)
-            grd = prob.getGradient(prob.gradCoeff)
-            [g2] = prob.dotProduct(grd, [grd])
-            prob.gradEps = max(0.001, np.sqrt(g2) / 10000)
-            cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False, epsInit=0.1)
-            req.result = {"at": prob.at, "xt": prob.xt, "obj": prob.obj, "iters": prob.iters,
-                          "converged": prob.converged, "calls": dict(prob.calls)}
+            with self._lane_context(lane):
+                prob = self._make_problem(req)
+                prob.lane = lane
+                with self.cv:
+                    lane.active.discard(slot)
+                    lane.active.add(prob)
+                    self.cv.notify_all()
+                # SurfaceMatching.optimizeMatching (surfaceMatching.py:474-484)
+                grd = prob.getGradient(prob.gradCoeff)
+                [g2] = prob.dotProduct(grd, [grd])
+                prob.gradEps = max(0.001, np.sqrt(g2) / 10000)
+                cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False, epsInit=0.1)
+                req.result = {"at": prob.at, "xt": prob.xt, "obj": prob.obj, "iters": prob.iters,
+                              "converged": prob.converged, "calls": dict(prob.calls)}
+                self._request_done(prob)
         except BaseException as exc:   # this request fails, the others go on
             req.error = exc
         finally:
             req.finish = time.perf_counter()
             with self.cv:
-                self.active.discard(prob)
+                lane.active.discard(slot)
+                lane.active.discard(prob)
+                self.n_active -= 1
                 self.hbm_in_use -= req.hbm_bytes()
                 self.finished.append(req)
                 self.cv.notify_all()
             req.done.set()
 
-    # -- engine side -----------------------------------------------------------------
+    def _request_done(self, prob):
+        """Hook: the request's last results are final (e.g. wait for its stream)."""
+
+    # -- admission (main thread) --------------------------------------------------------
     def _admit(self, now):
         start = []
         with self.cv:
@@ -285,7 +331,7 @@ class Scheduler:
                     req.start = req.finish = now
                     self.finished.append(req)
                     req.done.set()
-                elif (len(self.active) + len(start) < self.max_active
+                elif (self.n_active + len(start) < self.max_active
                       and self.hbm_in_use + req.hbm_bytes() <= self.hbm_budget):
                     self.hbm_in_use += req.hbm_bytes()
                     self.peak_hbm = max(self.peak_hbm, self.hbm_in_use)
@@ -293,71 +339,82 @@ class Scheduler:
                 else:
                     keep.append(req)
             self.queue = keep
-        for req in start:
-            req.start = time.perf_counter()
-            try:
-                prob = self._make_problem(req)
-            except BaseException as exc:
-                req.error = exc
-                req.finish = time.perf_counter()
-                with self.cv:
-                    self.hbm_in_use -= req.hbm_bytes()
-                    self.finished.append(req)
-                req.done.set()
-                continue
-            with self.cv:
-                self.active.add(prob)
-                self.max_active_seen = max(self.max_active_seen, len(self.active))
-            th = threading.Thread(target=self._run_request, args=(prob,), daemon=True)
-            self.threads.append(th)
-            th.start()
+            for req in start:
+                lane = self._lane_of(req)
+                slot = object()
+                lane.active.add(slot)
+                self.n_active += 1
+                self.max_active_seen = max(self.max_active_seen, self.n_active)
+                req.start = time.perf_counter()
+                th = threading.Thread(target=self._run_request, args=(req, lane, slot), daemon=True)
+                self.threads.append(th)
+                th.start()
+        return len(start)
 
     def _can_admit(self, now):
         if not self.queue or self.queue[0].arrival > now:
             return False
         req = self.queue[0]
-        return (len(self.active) < self.max_active
+        return (self.n_active < self.max_active
                 and (self.hbm_in_use + req.hbm_bytes() <= self.hbm_budget or req.hbm_bytes() > self.hbm_budget))
 
+    # -- lanes ------------------------------------------------------------------------------
+    def _lane_loop(self, lane):
+        with self._lane_context(lane):
+            while True:
+                with self.cv:
+                    while not (lane.active and len(lane.pending) == len(lane.active)) and not self._stop:
+                        self.cv.wait()
+                    if not (lane.active and len(lane.pending) == len(lane.active)):
+                        return
+                    ready = lane.pending
+                    lane.pending = {}
+                t0 = time.perf_counter()
+                self._execute(ready)
+                with self.stats_lock:
+                    self.busy_seconds += time.perf_counter() - t0
+                    self.rounds += 1
+                    lane.rounds += 1
+
     def run(self):
-        """Serves until the queue (including future arrivals) and the active set are empty."""
-        while True:
-            self._admit(time.perf_counter())
-            with self.cv:
-                if not self.active and not self.queue:
-                    break
-                ready = None
-                while True:
-                    if self.active and len(self.pending) == len(self.active):
-                        ready = self.pending
-                        self.pending = {}
+        """Serves until the queue (including future arrivals) and every lane are empty."""
+        self._stop = False
+        for lane in self.lanes:
+            lane.thread = threading.Thread(target=self._lane_loop, args=(lane,), daemon=True)
+            lane.thread.start()
+        try:
+            while True:
+                self._admit(time.perf_counter())
+                with self.cv:
+                    if self.n_active == 0 and not self.queue:
                         break
                     now = time.perf_counter()
                     if self._can_admit(now):
-                        break
+                        continue
                     nxt = self.queue[0].arrival if self.queue else None
-                    if not self.active and nxt is None:
-                        break
                     wait = None if (nxt is None or nxt <= now) else nxt - now
                     self.cv.wait(timeout=wait)
-            if ready:
-                t0 = time.perf_counter()
-                self._execute(ready)
-                self.busy_seconds += time.perf_counter() - t0
-                self.rounds += 1
-        # every request thread has finished its work; let them exit
-        for th in self.threads:
-            th.join()
-        self.threads = []
+        finally:
+            with self.cv:
+                self._stop = True
+                self.cv.notify_all()
+            for lane in self.lanes:
+                lane.thread.join()
+            # every request thread has finished its work; let them exit
+            for th in self.threads:
+                th.join()
+            self.threads = []
 
     def _execute(self, ready):
         groups = {}
         for prob, (kind, payload) in ready.items():
             groups.setdefault((kind, prob.req.group), []).append((prob, payload))
-        self.batch_sizes.append(len(ready))
+        with self.stats_lock:
+            self.batch_sizes.append(len(ready))
         out = {}
         for (kind, _), items in groups.items():
-            self.launches[kind] += 1
+            with self.stats_lock:
+                self.launches[kind] += 1
             fn = getattr(self, "_do_" + kind)
             try:
                 res = fn(items)
@@ -380,7 +437,8 @@ class Scheduler:
     def stats(self):
         lat = np.array([r.latency() for r in self.finished if r.error is None])
         return {"finished": len(self.finished), "failed": sum(r.error is not None for r in self.finished),
-                "rounds": self.rounds, "launch_groups": dict(self.launches),
+                "rounds": self.rounds, "lane_rounds": [l.rounds for l in self.lanes],
+                "launch_groups": dict(self.launches),
                 "mean_batch": float(np.mean(self.batch_sizes)) if self.batch_sizes else 0.0,
                 "max_batch": int(max(self.batch_sizes)) if self.batch_sizes else 0,
                 "max_active": self.max_active_seen, "peak_hbm_bytes": self.peak_hbm,
@@ -389,21 +447,43 @@ class Scheduler:
 
 
 class ServingEngine(Scheduler):
-    """Continuous-batching matcher on the current CUDA device (default stream):
-    submit() from any thread, run() drives the GPU.  line_search_precision:
-    'fp32c' (default) or 'fp64' data-term values, see the module docstring."""
+    """Continuous-batching matcher on the current CUDA device: submit() from any
+    thread, run() drives the GPU.
 
-    def __init__(self, hbm_budget_bytes=150e9, max_active=64, line_search_precision="fp32c"):
+    Each lane (size class, see Scheduler) launches on its own CUDA stream; the
+    lane of the smallest requests has the highest stream priority, so the
+    block scheduler runs its short kernels between the blocks of the large
+    requests' sweeps.  line_search_precision: 'fp32c' (default) or 'fp64'
+    data-term values, see the module docstring."""
+
+    def __init__(self, hbm_budget_bytes=150e9, max_active=64, line_search_precision="fp32c",
+                 lanes=(5000, 16000)):
         require_cuda()
         _lib.load()
         if line_search_precision not in ("fp32c", "fp64"):
             raise ValueError("line_search_precision must be 'fp32c' or 'fp64'")
-        super().__init__(hbm_budget_bytes, max_active)
+        super().__init__(hbm_budget_bytes, max_active, lanes)
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.lsp = line_search_precision
+        least, greatest = torch.cuda.Stream.priority_range()
+        nl = len(self.lanes)
+        for lane in self.lanes:
+            prio = max(greatest, least - (nl - 1 - lane.idx))
+            lane.stream = torch.cuda.Stream(device=self.device, priority=prio)
+
+    def _lane_context(self, lane):
+        return torch.cuda.stream(lane.stream)
 
     def _make_problem(self, req):
         return _Problem(req, self)
+
+    def run(self):
+        # the lanes' streams start after everything queued on the caller's stream
+        for lane in self.lanes:
+            lane.stream.wait_stream(torch.cuda.current_stream())
+        super().run()
+        for lane in self.lanes:
+            torch.cuda.current_stream().wait_stream(lane.stream)
 
     # -- ragged operations -----------------------------------------------------------------
     def _dataterm(self, probs, verts, grad, precision, target_self=False):

@@ -188,6 +188,22 @@ def test_groups_never_share_a_launch_and_failures_are_isolated():
         assert r.error is None and r.result["obj"] == _alone(r).result["obj"]
 
 
+def test_lanes_split_rounds_by_size_and_keep_results():
+    reqs = [_ToyRequest(i, n) for i, n in enumerate([4, 40, 5, 60, 6, 80])]
+    eng = _ToyEngine(lanes=(10, 50))
+    for r in reqs:
+        eng.submit(r)
+    eng.run()
+    st = eng.stats()
+    assert st["failed"] == 0 and all(n > 0 for n in st["lane_rounds"])
+    bounds = [10, 50, float("inf")]
+    for kind, rids, _ in eng.launch_log:
+        lanes = {next(k for k, b in enumerate(bounds) if reqs[i].n <= b) for i in rids}
+        assert len(lanes) == 1          # a launch never mixes lanes
+    for r in reqs:
+        assert r.result["obj"] == _alone(r).result["obj"]
+
+
 def test_latency_percentiles_reported():
     reqs = [_ToyRequest(i, 4) for i in range(5)]
     eng = _ToyEngine()
