@@ -197,6 +197,22 @@ LDDMM_API int lddmm_dataterm_f64(int cell_size, int norm, const double* vertices
                                  double eps2, double* energy, const int64_t* vertex_ptr, const int64_t* vertex_idx,
                                  double* px, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
+/* ---- dense-weight kernel sums: kff.applykmat / kff.applykdiffmat ---------------
+ * Replace py-lddmm/kernelFunctions.f90:499-552 and :554-610 (called by
+ * Kernel.applyK(matrixWeights=True), kernelFunctions.py:310-329, and
+ * Kernel.applyDiffKmat, kernelFunctions.py:405-410):
+ *   applykmat:     f[k,:] = sum_l K(x_k, y_l) beta[k,l,:]       beta (n, m, dimb), dimb <= 8
+ *   applykdiffmat: f[k,:] = sum_l K'(x_k, y_l) 2 (x_k - y_l) beta[k,l]   beta (n, m), f (n, d)
+ * x: targets (n, d), y: sources (m, d).  HBM-bound on beta; no workspace. */
+LDDMM_API int lddmm_applykmat_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d,
+                                   int dimb, double sigma, int order, double* f, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykmat_f64(const double* x, int64_t n, const double* y, int64_t m, const double* beta, int d,
+                                  int dimb, double sigma, int order, double* f, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiffmat_f32c(const double* x, int64_t n, const double* y, int64_t m, const double* beta,
+                                       int d, double sigma, int order, double* f, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiffmat_f64(const double* x, int64_t n, const double* y, int64_t m, const double* beta,
+                                      int d, double sigma, int order, double* f, lddmm_stream_t stream);
+
 /* ---- ragged launches: many independent problems in one launch ----------------
  * No single counterpart in the reference (which solves one problem per process);
  * each segment computes exactly what the single-problem entry point above

@@ -52,6 +52,10 @@ SIGNATURES = {
     "lddmm_epdiff_f64_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_epdiff_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _I, _P, _P, _P, _SZ, _P]),
     "lddmm_epdiff_f64": (_I, [_P, _I64, _I, _P, _I, _D, _I, _P, _P, _P, _SZ, _P]),
+    "lddmm_applykmat_f32c": (_I, [_P, _I64, _P, _I64, _P, _I, _I, _D, _I, _P, _P]),
+    "lddmm_applykmat_f64": (_I, [_P, _I64, _P, _I64, _P, _I, _I, _D, _I, _P, _P]),
+    "lddmm_applykdiffmat_f32c": (_I, [_P, _I64, _P, _I64, _P, _I, _D, _I, _P, _P]),
+    "lddmm_applykdiffmat_f64": (_I, [_P, _I64, _P, _I64, _P, _I, _D, _I, _P, _P]),
     # ragged launches: offset / sigma / regweight arguments are host arrays
     "lddmm_ragged_shoot_f32c_workspace": (_SZ, [_I, _P, _I, _I, _I]),
     "lddmm_ragged_shoot_f32c": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _P, _SZ, _P]),

@@ -159,7 +159,39 @@ class Kernel(KernelSpec):
         return output_like(x, f)
 
     def _applykmat(self, x, a, firstVar):
-        raise NotImplementedError("matrixWeights=True is provided by the fused varifold kernels")
+        """f_k = sum_l K(y_k, x_l) a[k, l, :] with dense weights a (N_targets, N, dimb)
+        (kernelFunctions.py:310-329 -> kff.applykmat, kernelFunctions.f90:499-552)."""
+        require_cuda()
+        src = to_dev(x)
+        tgt = src if firstVar is None else to_dev(firstVar)
+        w = to_dev(a)
+        n, m, d = tgt.shape[0], src.shape[0], src.shape[1]
+        if w.dim() != 3 or w.shape[0] != n or w.shape[1] != m:
+            raise ValueError("applyK(matrixWeights=True): a must be (N_targets, N_sources, dimb)")
+        dimb = w.shape[2]
+        if self.name == 'none':
+            return output_like(x, torch.zeros((n, dimb), dtype=torch.float64, device=src.device))
+        f = torch.empty((n, dimb), dtype=torch.float64, device=src.device)
+        _lib.call("lddmm_applykmat_" + _suffix(self.precision), ptr(tgt), n, ptr(src), m, ptr(w.contiguous()), d,
+                  dimb, float(self.sigma), int(self.order), ptr(f), stream_handle())
+        return output_like(x, f)
+
+    def applyDiffKmat(self, x, beta, firstVar=None):
+        """f_k = sum_l K'(y_k, x_l) 2 (y_k - x_l) beta[k, l] with dense beta (N_targets, N)
+        (kernelFunctions.py:405-410 -> kff.applykdiffmat, kernelFunctions.f90:554-610)."""
+        require_cuda()
+        src = to_dev(x)
+        tgt = src if firstVar is None else to_dev(firstVar)
+        b = to_dev(beta)
+        n, m, d = tgt.shape[0], src.shape[0], src.shape[1]
+        if b.dim() != 2 or b.shape[0] != n or b.shape[1] != m:
+            raise ValueError("applyDiffKmat: beta must be (N_targets, N_sources)")
+        if self.name == 'none':
+            return output_like(x, torch.zeros((n, d), dtype=torch.float64, device=src.device))
+        f = torch.empty((n, d), dtype=torch.float64, device=src.device)
+        _lib.call("lddmm_applykdiffmat_" + _suffix(self.precision), ptr(tgt), n, ptr(src), m, ptr(b.contiguous()),
+                  d, float(self.sigma), int(self.order), ptr(f), stream_handle())
+        return output_like(x, f)
 
 
 def _stack(a):

@@ -108,9 +108,20 @@ def dense_applydifft(R, kname, sigma, order, x, y, a1, a2):
     return 2 * (x * g1.sum(axis=1)[:, None] - g1 @ y)
 
 
+def dense_kmat(R, kname, sigma, order, x, y, diff=False):
+    """The reference's dense kernel matrix (or K' matrix with diff=True)."""
+    kf = R["kernelFunctions"]
+    if kname == "gauss":
+        K, _ = kf.kernelMatrixGauss(y, firstVar=x, par=[sigma], diff=diff)
+    else:
+        K, _ = kf.kernelMatrixLaplacian(y, firstVar=x, par=[sigma, order], diff=diff)
+    return K
+
+
 def kernel_cases(R, out):
     kf = R["kernelFunctions"]
     rng = np.random.default_rng(1234)
+    rng_mat = np.random.default_rng(4321)   # dense-weight cases (separate stream)
     cases = []
     for kname, order in [("gauss", 10), ("laplacian", 0), ("laplacian", 1), ("laplacian", 2), ("laplacian", 3),
                          ("laplacian", 4)]:
@@ -135,6 +146,19 @@ def kernel_cases(R, out):
                 out["applyk_dense_" + tag] = dense_applyk(R, kname, sigma, K.order, x, y, beta)
                 out["applyk_exact_" + tag] = oracle.applyk(x, y, beta, sigma, K.order)
                 oracle.set_exact_coeffs(False)
+                # dense weights: Kernel.applyK(matrixWeights=True) -> kff.applykmat
+                bmat = rng_mat.standard_normal((n, m, dimb))
+                out["kmat_b_" + tag] = bmat
+                out["kmat_f_" + tag] = K.applyK(y, bmat, firstVar=x, matrixWeights=True)
+                Kd = dense_kmat(R, kname, sigma, K.order, x, y)
+                out["kmat_dense_" + tag] = (Kd[:, :, None] * bmat).sum(axis=1)
+                if K.order > 0 and dimb == 1:
+                    # Kernel.applyDiffKmat -> kff.applykdiffmat
+                    b2 = rng_mat.standard_normal((n, m))
+                    out["kdiffmat_b_" + tag] = b2
+                    out["kdiffmat_f_" + tag] = K.applyDiffKmat(y, b2, firstVar=x)
+                    g = dense_kmat(R, kname, sigma, K.order, x, y, diff=True) * b2
+                    out["kdiffmat_dense_" + tag] = 2 * (x * g.sum(axis=1)[:, None] - g @ y)
                 if K.order > 0:
                     for na in (1, 3):
                         a1 = rng.standard_normal((na, n, dimb))

@@ -48,6 +48,43 @@ def test_golden_cases_applyk_difft(golden, oracle_lib, kf, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+def test_golden_cases_dense_weights(golden, kf, precision):
+    """Kernel.applyK(matrixWeights=True) / applyDiffKmat (kff.applykmat /
+    applykdiffmat) against the reference outputs of every golden kernel case."""
+    for tag in golden["kernel_cases"]:
+        tag = str(tag)
+        name = "gauss" if tag.startswith("gauss") else "laplacian"
+        order = int(tag.split("_")[0].replace(name, ""))
+        K = kf.Kernel(name=name, sigma=0.35, order=order, precision=precision)
+        x, y = golden["applyk_x_" + tag], golden["applyk_y_" + tag]
+        f = K.applyK(y, golden["kmat_b_" + tag], firstVar=x, matrixWeights=True)
+        assert isinstance(f, np.ndarray) and f.shape == golden["kmat_f_" + tag].shape
+        assert _err(f, golden["kmat_f_" + tag]) < TOL[precision], (tag, precision)
+        if "kdiffmat_b_" + tag in golden.files:
+            fd = K.applyDiffKmat(y, golden["kdiffmat_b_" + tag], firstVar=x)
+            assert _err(fd, golden["kdiffmat_f_" + tag]) < TOL[precision], (tag, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("n,m,dimb", [(1, 1, 1), (700, 1300, 1), (1500, 900, 3)])
+def test_dense_weights_random_sizes(oracle_lib, kf, precision, n, m, dimb):
+    rng = np.random.default_rng(n + m + dimb)
+    x = rng.uniform(0, 1, (n, 3))
+    y = rng.uniform(0, 1, (m, 3))
+    b = rng.standard_normal((n, m, dimb))
+    for name, order, sigma in [("gauss", 10, 0.1), ("laplacian", 3, 0.1)]:
+        K = kf.Kernel(name=name, sigma=sigma, order=order, precision=precision)
+        f = K.applyK(y, b, firstVar=x, matrixWeights=True)
+        assert _err(f, oracle_lib.applykmat(x, y, b, sigma, K.order)) < TOL[precision]
+        fd = K.applyDiffKmat(y, b[:, :, 0], firstVar=x)
+        assert _err(fd, oracle_lib.applykdiffmat(x, y, b[:, :, 0], sigma, K.order)) < TOL[precision]
+    # self-interaction form (firstVar=None): targets = sources
+    b2 = rng.standard_normal((m, m, dimb))
+    K = kf.Kernel(name="gauss", sigma=0.1, precision=precision)
+    assert _err(K.applyK(y, b2, matrixWeights=True), oracle_lib.applykmat(y, y, b2, 0.1, 10)) < TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
 @pytest.mark.parametrize("name,order,sigma", [("gauss", 10, 0.05), ("laplacian", 3, 0.05), ("laplacian", 1, 0.1)])
 @pytest.mark.parametrize("n,m", [(1, 1), (1000, 1), (3001, 5003), (20000, 777)])
 def test_random_sizes_against_oracle(oracle_lib, kf, precision, name, order, sigma, n, m):

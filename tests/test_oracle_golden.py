@@ -49,6 +49,35 @@ def test_loops_reproduce_reference_dispatch(golden, oracle_lib):
                                                             firstVar=x), golden["difft_f_" + k])
 
 
+def test_dense_weight_loops_match_reference_dense_matrices(golden, oracle_lib):
+    """kff.applykmat / applykdiffmat (restated) against the reference's dense
+    kernel matrices times the weights, and the reference's dispatch
+    (Kernel.applyK(matrixWeights=True), Kernel.applyDiffKmat) == oracle calls."""
+    for tag in golden["kernel_cases"]:
+        tag = str(tag)
+        name = "gauss" if tag.startswith("gauss") else "laplacian"
+        order = int(tag.split("_")[0].replace(name, ""))
+        x, y = golden["applyk_x_" + tag], golden["applyk_y_" + tag]
+        b = golden["kmat_b_" + tag]
+        tol = 1e-13 if "laplacian0" not in tag else 2e-9
+        oracle_lib.set_exact_coeffs(True)
+        try:
+            assert _rel(oracle_lib.applykmat(x, y, b, 0.35, order), golden["kmat_dense_" + tag]) < tol, tag
+            if "kdiffmat_b_" + tag in golden.files:
+                b2 = golden["kdiffmat_b_" + tag]
+                assert _rel(oracle_lib.applykdiffmat(x, y, b2, 0.35, order),
+                            golden["kdiffmat_dense_" + tag]) < 1e-13, tag
+        finally:
+            oracle_lib.set_exact_coeffs(False)
+        assert _rel(golden["kmat_f_" + tag], golden["kmat_dense_" + tag]) < 5e-8, tag
+        K = ref.Kernel(name=name, sigma=0.35, order=order)
+        np.testing.assert_array_equal(K.applyK(y, b, firstVar=x, matrixWeights=True), golden["kmat_f_" + tag])
+        if "kdiffmat_b_" + tag in golden.files:
+            b2 = golden["kdiffmat_b_" + tag]
+            assert _rel(golden["kdiffmat_f_" + tag], golden["kdiffmat_dense_" + tag]) < 1e-7, tag
+            np.testing.assert_array_equal(K.applyDiffKmat(y, b2, firstVar=x), golden["kdiffmat_f_" + tag])
+
+
 def test_laplacian_order0_derivative_rejected(oracle_lib):
     x = np.zeros((2, 3))
     with pytest.raises(ValueError):
