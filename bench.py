@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=512, help="requests of the serving stream")
     ap.add_argument("--sigma-error", type=float, default=None, help="sigmaError of the matching workloads")
     ap.add_argument("--max-active", type=int, default=64, help="serving slots")
+    ap.add_argument("--line-search", default="auto", choices=["auto", "fp64", "fp32c"],
+                    help="precision of the data-term values compared by the served line search")
     ap.add_argument("--lanes", default="5000,16000",
                     help="serving size-class bounds (vertex counts), comma separated, or 'none'")
     return ap.parse_args()
@@ -302,25 +304,30 @@ def run_curve(args):
     from registration_b200 import curves as cv
     from registration_b200 import kernelFunctions as kf
 
-    def match(precision):
+    def match(precision, lsp=None):
         param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
                                       KparDist=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
                                       sigmaError=sig_err, errorType="current")
         cm = CM.CurveMatching(Template=cv.Curve(pointSet=v), Target=cv.Curve(pointSet=vt), param=param,
-                              maxIter=iters, saveRate=0)
+                              maxIter=iters, saveRate=0,
+                              lineSearchPrecision=lsp or ("auto" if precision == "fp32c" else precision))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         cm.optimizeMatching()
         torch.cuda.synchronize()
         return time.perf_counter() - t0, cm
 
+    # headline: FP32c kernel sums, FP64 reductions, the 'auto' line search
+    # (FP32c data-term values refined to FP64 where a comparison needs it);
+    # beside it FP32c with FP64 line-search values and the plain FP64 path
     for _ in range(max(1, args.warmup)):
         match("fp32c")
     times = []
     for _ in range(args.steps):
         dt_, cm = match("fp32c")
         times.append(dt_)
-    _, cm64 = match("fp64")
+    t_ls64, cm_ls64 = match("fp32c", "fp64")
+    t64, cm64 = match("fp64")
     cpu = None
     if not args.no_cpu_baseline:
         import oracle
@@ -339,7 +346,10 @@ def run_curve(args):
     val = 1.0 / float(np.mean(times))
     _line(args, "curve matches/s", val, "matches/s", True, config,
           {"ms_per_step": 1e3 * float(np.mean(times)), "final_energy_fp32c": cm.obj, "final_energy_fp64": cm64.obj,
-           "final_energy_abs_diff": abs(cm.obj - cm64.obj), "iterations": cm.iter, "calls": cm.calls,
+           "final_energy_abs_diff": abs(cm.obj - cm64.obj), "iterations": cm.iter, "iterations_fp64": cm64.iter,
+           "calls": cm.calls, "fp64_gpu_ms": 1e3 * t64,
+           "fp32c_with_fp64_line_search": {"ms": 1e3 * t_ls64, "final_energy": cm_ls64.obj,
+                                           "iterations": cm_ls64.iter},
            "cpu_baseline": cpu,
            "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": int(v.nbytes + vt.nbytes),
                    "d2h_bytes_per_step": int(cm.at.numel() * 8)}})
@@ -359,24 +369,29 @@ def run_surface(args):
     from registration_b200 import surfaceMatching as SM
     from registration_b200 import surfaces as sf
 
-    def match(precision, maxit):
+    def match(precision, maxit, lsp=None):
         param = SM.SurfaceMatchingParam(timeStep=0.1,
                                         KparDiff=kf.Kernel(name="gauss", sigma=0.2, precision=precision),
                                         KparDist=kf.Kernel(name="gauss", sigma=0.1, precision=precision),
                                         sigmaError=sig_err, errorType="varifold")
         sm = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v]), Target=sf.Surface(FV=[f, vt]), param=param,
-                                maxIter=maxit, testGradient=False)
+                                maxIter=maxit, testGradient=False,
+                                lineSearchPrecision=lsp or ("auto" if precision == "fp32c" else precision))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sm.optimizeMatching()
         torch.cuda.synchronize()
         return time.perf_counter() - t0, sm
 
+    # headline: FP32c kernel sums, FP64 reductions, 'auto' line search (FP32c
+    # data-term values refined to FP64 where a comparison needs it); beside it
+    # FP32c with FP64 line-search values and plain FP64
     match("fp32c", 3)   # warm-up (library load, workspaces)
     times = []
     for _ in range(args.steps):
         dt_, sm = match("fp32c", iters)
         times.append(dt_)
+    t_ls64, sm_ls64 = match("fp32c", iters, "fp64")
     t64, sm64 = match("fp64", iters)
     cpu = None
     if not args.no_cpu_baseline:
@@ -386,7 +401,10 @@ def run_surface(args):
           {"ms_per_step": 1e3 * float(np.mean(times)), "ms_per_iteration": 1e3 * float(np.mean(times)) / max(1, sm.iter),
            "final_energy_fp32c": sm.obj, "final_energy_fp64": sm64.obj,
            "final_energy_abs_diff": abs(sm.obj - sm64.obj), "iterations": sm.iter, "iterations_fp64": sm64.iter,
-           "fp64_gpu_ms": 1e3 * t64, "calls": sm.calls, "cpu_baseline": cpu,
+           "fp64_gpu_ms": 1e3 * t64, "calls": sm.calls,
+           "fp32c_with_fp64_line_search": {"ms": 1e3 * t_ls64, "final_energy": sm_ls64.obj,
+                                           "iterations": sm_ls64.iter},
+           "cpu_baseline": cpu,
            "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": int(v.nbytes + vt.nbytes + f.nbytes),
                    "d2h_bytes_per_step": int(sm.at.numel() * 8)}})
     return 0
@@ -587,7 +605,7 @@ def run_serving(args):
     sig_err = args.sigma_error if args.sigma_error is not None else 0.01
     R = args.requests
     lanes = () if args.lanes in ("", "none") else tuple(int(b) for b in args.lanes.split(","))
-    ekw = {"max_active": args.max_active, "lanes": lanes}
+    ekw = {"max_active": args.max_active, "lanes": lanes, "line_search_precision": args.line_search}
     t_prep = time.perf_counter()
     stream = serving_stream(R, args.seed, iters, sig_err)
     t_prep = time.perf_counter() - t_prep
@@ -595,7 +613,8 @@ def run_serving(args):
     config = {"workload": "served surface matching: %d requests, V ~ logU[2000, 50000] icosphere-derived, 4-16 "
                           "bumps, gauss sigma ~ U[0.05, 0.3], varifold sigma = sigma/2, sigmaError %g, T 10, %d cg "
                           "iterations max, Poisson arrivals at 80%% of measured capacity, %d slots, 150 GB HBM "
-                          "budget, size lanes %s" % (R, sig_err, iters, args.max_active, list(lanes))}
+                          "budget, size lanes %s, line search %s" % (R, sig_err, iters, args.max_active, list(lanes),
+                                                                     args.line_search)}
     # warm-up: library load, workspace growth, cuBLAS handles
     warm = _fresh([stream[int(np.argmin(sizes))]])
     for r in warm:
@@ -714,6 +733,8 @@ def run_serving(args):
            "mean_batch": st["mean_batch"], "max_batch": st["max_batch"], "max_active": st["max_active"],
            "lane_rounds": st["lane_rounds"],
            "iterations_mean": float(its.mean()), "iterations_min": int(its.min()),
+           "value_refinements": int(sum(r.result["calls"].get("refine", 0) for r in ok)),
+           "values": int(sum(r.result["calls"]["value"] for r in ok)),
            "converged": int(sum(r.result["converged"] for r in ok)),
            "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
            "one_at_a_time_fp64_gpu": {"matches_per_s": base_thr, "seconds_per_stream": pred,

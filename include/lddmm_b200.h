@@ -250,14 +250,20 @@ LDDMM_API int lddmm_ragged_applyk_f32c(int nseg, const int64_t* t_start, const i
  * request s owns vertices [v_off[s], v_off[s+1]), cells [c_off[s], c_off[s+1])
  * (entries are GLOBAL vertex indices) and target cells [c2_off[s], c2_off[s+1]);
  * vertex_ptr (v_off[nreq]+1) / vertex_idx (c_off[nreq]*cell_size, entries
- * global cell*cell_size+corner) is the concatenated incidence; energy[nreq]. */
+ * global cell*cell_size+corner) is the concatenated incidence; energy[nreq].
+ * frame: NULL (each request is packed relative to the centre of the bounding box
+ * of its cells, as the single-problem entry points do) or a HOST array
+ * (nreq, 3) of fixed packing centres -- with a fixed centre the FP32 rounding
+ * of the target cells is the same in every call, so differences of values
+ * between calls (line searches) do not carry it. */
 LDDMM_API size_t lddmm_ragged_dataterm_f32c_workspace(int nreq, int cell_size, int norm, const int64_t* v_off,
                                                       const int64_t* c_off, const int64_t* c2_off, int d, int order,
                                                       int want_energy, int want_grad);
 LDDMM_API int lddmm_ragged_dataterm_f32c(int nreq, int cell_size, int norm, const int64_t* v_off,
                                          const int64_t* c_off, const int64_t* c2_off, const double* vertices, int d,
                                          const int64_t* cells, const double* tgt_centers, const double* tgt_vectors,
-                                         const double* sigma, int order, double eps1, double eps2, double* energy,
+                                         const double* sigma, int order, double eps1, double eps2,
+                                         const double* frame, double* energy,
                                          const int64_t* vertex_ptr, const int64_t* vertex_idx, double* px,
                                          void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 LDDMM_API size_t lddmm_ragged_dataterm_f64_workspace(int nreq, int cell_size, int norm, const int64_t* v_off,
@@ -266,7 +272,8 @@ LDDMM_API size_t lddmm_ragged_dataterm_f64_workspace(int nreq, int cell_size, in
 LDDMM_API int lddmm_ragged_dataterm_f64(int nreq, int cell_size, int norm, const int64_t* v_off,
                                         const int64_t* c_off, const int64_t* c2_off, const double* vertices, int d,
                                         const int64_t* cells, const double* tgt_centers, const double* tgt_vectors,
-                                        const double* sigma, int order, double eps1, double eps2, double* energy,
+                                        const double* sigma, int order, double eps1, double eps2,
+                                         const double* frame, double* energy,
                                         const int64_t* vertex_ptr, const int64_t* vertex_idx, double* px,
                                         void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 

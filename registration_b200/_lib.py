@@ -66,9 +66,9 @@ SIGNATURES = {
     "lddmm_ragged_dataterm_f32c_workspace": (_SZ, [_I, _I, _I, _P, _P, _P, _I, _I, _I, _I]),
     "lddmm_ragged_dataterm_f64_workspace": (_SZ, [_I, _I, _I, _P, _P, _P, _I, _I, _I, _I]),
     "lddmm_ragged_dataterm_f32c": (_I, [_I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _I, _D, _D, _P, _P, _P, _P,
-                                        _P, _SZ, _P]),
+                                        _P, _P, _SZ, _P]),
     "lddmm_ragged_dataterm_f64": (_I, [_I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _I, _D, _D, _P, _P, _P, _P,
-                                       _P, _SZ, _P]),
+                                       _P, _P, _SZ, _P]),
 }
 
 ERRORS = {-1: "invalid argument", -2: "workspace too small", -3: "CUDA error", -4: "unsupported"}

@@ -8,12 +8,15 @@ every objective value and dot product is reduced in FP64 on the device and
 read back as one host double, which is what the line search compares.
 
 Precision: kernel sums (shooting, adjoint, data-term gradient, dot products)
-follow the kernels' own precision.  The data-term VALUE that the line search
-compares is evaluated with an FP64 copy of KparDist by default
-(lineSearchPrecision='fp64'): the reference's stop test is an absolute
+follow the kernels' own precision.  The reference's stop test is an absolute
 |obj - objTry| < 1e-6 on objectives that are differences of norms of order
-|S|^2 (1e2 for a unit sphere at sigmaError 0.5), i.e. ~1e-9 relative, which an
-FP32 pair evaluation (~3e-7 relative error per term) cannot resolve.
+|S|^2 (1e2 for a unit sphere at sigmaError 0.5), i.e. ~1e-9 relative, which
+FP32 pair evaluation cannot always resolve.  lineSearchPrecision selects the
+data-term VALUE that the line search compares:
+  'fp64' (default): an FP64 copy of KparDist for every value;
+  'auto': KparDist's own precision with an error bound, refined to FP64 only
+      when a comparison cannot be decided (registration_b200._precision);
+  'fp32c' / KparDist's precision: no refinement.
 
 Two reuses that do not change any value: the trajectory of an accepted trial
 step is kept instead of re-shooting it in endOfIteration, and getGradient
@@ -28,6 +31,7 @@ import torch
 
 from . import _dataterm as _dt
 from . import pointEvolution as evol
+from ._precision import _Value, value_bound
 from .device import require_cuda, to_dev
 
 
@@ -41,7 +45,8 @@ class Direction:
 class DeviceMatching:
     """Subclasses set: fv0, fv1 (shapes), param, norm_name, tgt_vectors_attr."""
 
-    def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision='fp64'):
+    def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision='fp64',
+                    noise=1e-8):
         require_cuda()
         if affine not in ('none', None):
             raise NotImplementedError("affine registration components are not provided (affine='none' only)")
@@ -75,7 +80,12 @@ class DeviceMatching:
         self.fvDef.updateVertices(self.x0)
         self._fast_data = self._our_norm_functions()
         K = self.param.KparDist
-        if lineSearchPrecision == K.precision:
+        self._auto = lineSearchPrecision == 'auto'
+        self._noise = float(noise)
+        self.noise_obs = 0.0
+        self._K64 = K if K.precision == 'fp64' else type(K)(name=K.name, sigma=K.sigma, order=K.order,
+                                                              weight=K.weight, precision='fp64')
+        if self._auto or lineSearchPrecision == K.precision:
             self._Kval = K
         else:
             self._Kval = type(K)(name=K.name, sigma=K.sigma, order=K.order, weight=K.weight,
@@ -93,16 +103,29 @@ class DeviceMatching:
                 getattr(mod, name + 'NormGradient', None))
         return (self.param.fun_obj0, self.param.fun_obj, self.param.fun_objGrad) == want
 
-    def _data_energy(self, vertices):
+    def _data_energy(self, vertices, K=None):
         """fun_obj(fvDef, fv1, KparDist) / sigmaError^2 as a device scalar."""
+        K = self._Kval if K is None else K
         if self._fast_data:
             e, _ = _dt.dataterm(self.param.errorType, vertices, self._dshape, self._tc, self._tv,
-                                self._Kval, energy=True, grad=False)
+                                K, energy=True, grad=False)
             return e / (self.param.sigmaError ** 2)
         ff = self.shape_copy(self.fvDef)
         ff.updateVertices(vertices)
-        return torch.tensor(self.param.fun_obj(ff, self.fv1, self._Kval) / self.param.sigmaError ** 2,
+        return torch.tensor(self.param.fun_obj(ff, self.fv1, K) / self.param.sigmaError ** 2,
                             dtype=torch.float64, device=self.x0.device)
+
+    def _trial_value(self, e_reg, x_end):
+        """obj0 + deformation energy + data term, as compared by the line search."""
+        v = self.obj0 + float(e_reg + self._data_energy(x_end))
+        if self._auto:
+            v = _Value(v, self, float(e_reg), x_end, value_bound(self, self._noise, self.obj0))
+        return v
+
+    def exact_value(self, ereg, x_end):
+        """The objective with an FP64 data-term value (refinement of a _Value)."""
+        self.calls["refine"] = self.calls.get("refine", 0) + 1
+        return self.obj0 + float(ereg + self._data_energy(x_end, self._K64))
 
     def dataTerm(self, _fvDef, _fvInit=None):
         return float(self._data_energy(to_dev(_fvDef.vertices)))
@@ -131,11 +154,12 @@ class DeviceMatching:
     def objectiveFun(self):
         """(surfaceMatching.py:233-250)"""
         if self.obj is None:
-            self.obj0 = self.param.fun_obj0(self.fv1, self._Kval) / (self.param.sigmaError ** 2)
+            K0 = self._K64 if self._auto else self._Kval
+            self.obj0 = self.param.fun_obj0(self.fv1, K0) / (self.param.sigmaError ** 2)
             xt, e = evol.shoot(self.x0, self.at, self.param.KparDiff, regweight=self.regweight, with_energy=True)
             self.xt = xt
             self.fvDef.updateVertices(xt[-1])
-            self.obj = float(e + self._data_energy(xt[-1])) + self.obj0
+            self.obj = self._trial_value(e, xt[-1])
         return self.obj
 
     def getVariable(self):
@@ -146,7 +170,7 @@ class DeviceMatching:
         self.calls["updateTry"] += 1
         atTry = self.at - eps * dir.diff
         xt, e = evol.shoot(self.x0, atTry, self.param.KparDiff, regweight=self.regweight, with_energy=True)
-        objTry = self.obj0 + float(e + self._data_energy(xt[-1]))
+        objTry = self._trial_value(e, xt[-1])
         if np.isnan(objTry):
             logging.info('Warning: nan in updateTry')
             return 1e500
@@ -206,4 +230,5 @@ class DeviceMatching:
         self.fvDef.updateVertices(self.xt[-1])
 
     def endOptim(self):
-        pass
+        if isinstance(self.obj, _Value):
+            self.obj = float(self.obj.refine())

@@ -670,6 +670,7 @@ struct RagDataArgs {
     const double* sigma;
     int order;
     double eps1, eps2;
+    const double* frame;   // host (nseg, 3) packing centres, or NULL: bounding-box centre per call
     double* energy;
     const int64_t* vptr;
     const int64_t* vidx;
@@ -706,13 +707,15 @@ int rag_dt_sweep(const RagDataArgs& a, int kind, int grad, double sign2, const d
         const KScale ks = kernel_scale<Real>(kind, a.order, a.sigma[s]);
         pl.segs[s].scale = ks.scale;
         pl.segs[s].dscale = ks.dscale;
+        if (a.frame)
+            for (int j = 0; j < 3; ++j) pl.segs[s].center[j] = j < a.d ? a.frame[3 * s + j] : 0.0;
     }
     const int nbb = rag_bbox_prepare(pl.segs, a.c2 != nullptr);
     LDDMM_TRY(rag_copy_table(pl.segs.data(), sizeof(RagSeg) * nseg, dsegs, st));
     LDDMM_TRY(rag_copy_table(pl.desc.data(), sizeof(SegDesc) * nseg, ddesc, st));
     LDDMM_TRY(rag_copy_table(padoff.data(), sizeof(long long) * (nseg + 1), dpad, st));
     LDDMM_TRY(rag_copy_table(rowoff.data(), sizeof(long long) * (nseg + 1), drow, st));
-    rag_bbox_launch<false>(dsegs, nseg, nbb, c1, a.c2, a.d, 0, st);
+    if (!a.frame) rag_bbox_launch<false>(dsegs, nseg, nbb, c1, a.c2, a.d, 0, st);
     typename Op::Params P{};
     P.src4 = src;
     P.src_stride = pl.ss;
@@ -1015,7 +1018,7 @@ int lddmm_ragged_applyk_f32c(int nseg, const int64_t* t_start, const int64_t* t_
 
 #define RAG_DT_BODY(REAL)                                                                                         \
     RagDataArgs a{nreq, cell_size, norm, v_off, c_off, c2_off, vertices, d, cells, tgt_centers, tgt_vectors,        \
-                  sigma, order, eps1, eps2, energy, vertex_ptr, vertex_idx, px};                                   \
+                  sigma, order, eps1, eps2, frame, energy, vertex_ptr, vertex_idx, px};                            \
     auto run = [&](Workspace& ws) {                                                                                 \
         return rag_dispatch_pq(order, [&](auto kind, auto pdeg, auto qdeg) {                                        \
             return dispatch_d(d, [&](auto D) {                                                                      \
@@ -1064,8 +1067,9 @@ static int rag_dt_validate(int nreq, int cell_size, int norm, const int64_t* v_o
 #define RAG_DT_SIG                                                                                              \
     int nreq, int cell_size, int norm, const int64_t *v_off, const int64_t *c_off, const int64_t *c2_off,        \
         const double *vertices, int d, const int64_t *cells, const double *tgt_centers, const double *tgt_vectors, \
-        const double *sigma, int order, double eps1, double eps2, double *energy, const int64_t *vertex_ptr,     \
-        const int64_t *vertex_idx, double *px, void *workspace, size_t workspace_bytes, lddmm_stream_t stream
+        const double *sigma, int order, double eps1, double eps2, const double *frame, double *energy,           \
+        const int64_t *vertex_ptr, const int64_t *vertex_idx, double *px, void *workspace, size_t workspace_bytes,  \
+        lddmm_stream_t stream
 
 #define RAG_DT_ENTRY(REAL, WHO)                                                                                    \
     LDDMM_TRY(rag_dt_validate(nreq, cell_size, norm, v_off, c_off, c2_off, d, sigma, order, vertices, cells,       \
@@ -1088,6 +1092,7 @@ int lddmm_ragged_dataterm_f64(RAG_DT_SIG) { RAG_DT_ENTRY(double, "ragged datater
     double* energy = want_energy ? reinterpret_cast<double*>(16) : nullptr;                                        \
     double* px = want_grad ? reinterpret_cast<double*>(16) : nullptr;                                              \
     double eps1 = 0, eps2 = 0;                                                                                     \
+    const double* frame = nullptr;                                                                                 \
     void* stream = nullptr;                                                                                        \
     RAG_DT_BODY(REAL)                                                                                              \
     Workspace ws;                                                                                                  \

@@ -24,11 +24,18 @@ decisions) depends only on that request's own data, so a request's result is
 bit-identical alone and in any mix.
 
 Precision: FP32 compensated kernel sums for shooting, the adjoint, the data
-term and the dot products; every energy and dot product is reduced in FP64 and
-the line search compares FP64 numbers.  ``line_search_precision='fp64'`` makes
-the data-term VALUES FP64 pair sums as well (the single-problem default, needed
-to reproduce the reference's iteration trace; it costs a full FP64 sweep per
-trial step).
+term and the dot products; every energy and dot product is reduced in FP64.
+The line search of the reference compares objective values down to an
+absolute 1e-6 (its stop test and its tiny `epsSmall` probe step), while the
+objective is a small difference of norms of order |S|^2 / sigmaError^2.
+``line_search_precision``:
+  'auto' (default): trial values use FP32c data-term sums and carry an error
+      bound; a comparison that the bounds cannot decide re-evaluates the data
+      term of both values in FP64 (registration_b200._precision), so every
+      decision is the one an FP64 evaluation takes;
+  'fp64': every trial value uses an FP64 data-term sweep;
+  'fp32c': no refinement (fastest; decisions between values closer than the
+      FP32c noise are arbitrary, which can end a run early).
 """
 import ctypes
 import threading
@@ -40,6 +47,7 @@ import torch
 from . import _dataterm as _dt
 from . import _lib
 from . import conjugateGradient as cg
+from ._precision import _Value, value_bound
 from .device import ptr, require_cuda, stream_handle, workspace
 
 NORMS = {"current": 0, "measure": 1, "varifold": 2}
@@ -141,6 +149,10 @@ class _Problem:
         c1, s1 = _dt.cell_geometry(req.v1, req.f1)
         self.tc = torch.from_numpy(np.ascontiguousarray(c1)).to(dev)
         self.tv = torch.from_numpy(np.ascontiguousarray(s1)).to(dev)
+        # fixed data-term packing frame: centre of the target cells' bounding box
+        lo, hi = c1.min(axis=0), c1.max(axis=0)
+        self.frame = tuple(float(0.5 * (lo[j] + hi[j])) if j < c1.shape[1] else 0.0 for j in range(3))
+        self.noise_obs = 0.0
         self.dshape = _dt.DeviceShape(req.f0, req.n)
         self.tshape = _dt.DeviceShape(req.f1, len(req.v1))
         self.at = torch.zeros((self.T, self.npt, self.dim), dtype=torch.float64, device=dev)
@@ -153,22 +165,32 @@ class _Problem:
         self.gradCoeff = self.npt
         self.converged = False
         self.iters = 0
-        self.calls = {"value": 0, "grad": 0, "dot": 0}
+        self.calls = {"value": 0, "grad": 0, "dot": 0, "refine": 0}
 
     def getVariable(self):
         return [self.at]
 
+    def _value(self, at):
+        """obj0 + deformation energy + data term / sigmaError^2 at momenta `at`."""
+        tot, ereg, xt = self.engine.post(self, "value", at)
+        v = self.obj0 + tot
+        if self.engine.lsp == "auto":
+            v = _Value(v, self, ereg, xt[-1], value_bound(self, self.engine.noise, self.obj0))
+        return v, xt
+
+    def exact_value(self, ereg, x_end):
+        """The same objective with an FP64 data-term value (one posted launch)."""
+        return self.obj0 + ereg + self.engine.post(self, "refine", x_end)
+
     def objectiveFun(self):
         if self.obj is None:
             self.obj0 = self.engine.post(self, "norm0", None)
-            e, self.xt = self.engine.post(self, "value", self.at)
-            self.obj = e + self.obj0
+            self.obj, self.xt = self._value(self.at)
         return self.obj
 
     def updateTry(self, dir, eps, objRef=None):
         atTry = self.at - eps * dir.diff
-        e, xt = self.engine.post(self, "value", atTry)
-        objTry = self.obj0 + e
+        objTry, xt = self._value(atTry)
         if np.isnan(objTry):
             return 1e500
         if (objRef is None) or (objTry < objRef):
@@ -243,7 +265,7 @@ class Scheduler:
         self.hbm_in_use = 0.0
         self.n_active = 0
         self.rounds = 0
-        self.launches = {"norm0": 0, "value": 0, "grad": 0, "dot": 0}
+        self.launches = {"norm0": 0, "value": 0, "grad": 0, "dot": 0, "refine": 0}
         self.batch_sizes = []
         self.busy_seconds = 0.0
         self.max_active_seen = 0
@@ -298,7 +320,8 @@ class Scheduler:
                 [g2] = prob.dotProduct(grd, [grd])
                 prob.gradEps = max(0.001, np.sqrt(g2) / 10000)
                 cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False, epsInit=0.1)
-                req.result = {"at": prob.at, "xt": prob.xt, "obj": prob.obj, "iters": prob.iters,
+                obj = prob.obj.refine() if isinstance(prob.obj, _Value) else float(prob.obj)
+                req.result = {"at": prob.at, "xt": prob.xt, "obj": obj, "iters": prob.iters,
                               "converged": prob.converged, "calls": dict(prob.calls)}
                 self._request_done(prob)
         except BaseException as exc:   # this request fails, the others go on
@@ -453,18 +476,26 @@ class ServingEngine(Scheduler):
     Each lane (size class, see Scheduler) launches on its own CUDA stream; the
     lane of the smallest requests has the highest stream priority, so the
     block scheduler runs its short kernels between the blocks of the large
-    requests' sweeps.  line_search_precision: 'fp32c' (default) or 'fp64'
-    data-term values, see the module docstring."""
+    requests' sweeps.  line_search_precision: 'auto' (default), 'fp64' or
+    'fp32c', see the module docstring; noise: the initial bound of the error
+    of a difference of two FP32c objective values, as a fraction of the
+    target's Norm0 / sigmaError^2 (measured near optima: ~1e-9 of it; the
+    bound grows with every error measured by a refinement); fixed_frame: pack
+    each request's data term relative to a fixed centre (the target's
+    bounding box), so values of different calls share the rounding of the
+    target cells."""
 
-    def __init__(self, hbm_budget_bytes=150e9, max_active=64, line_search_precision="fp32c",
-                 lanes=(5000, 16000)):
+    def __init__(self, hbm_budget_bytes=150e9, max_active=64, line_search_precision="auto",
+                 lanes=(5000, 16000), fixed_frame=True, noise=1e-8):
         require_cuda()
         _lib.load()
-        if line_search_precision not in ("fp32c", "fp64"):
-            raise ValueError("line_search_precision must be 'fp32c' or 'fp64'")
+        if line_search_precision not in ("auto", "fp32c", "fp64"):
+            raise ValueError("line_search_precision must be 'auto', 'fp32c' or 'fp64'")
         super().__init__(hbm_budget_bytes, max_active, lanes)
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.lsp = line_search_precision
+        self.fixed_frame = bool(fixed_frame)
+        self.noise = float(noise)
         least, greatest = torch.cuda.Stream.priority_range()
         nl = len(self.lanes)
         for lane in self.lanes:
@@ -486,7 +517,7 @@ class ServingEngine(Scheduler):
             torch.cuda.current_stream().wait_stream(lane.stream)
 
     # -- ragged operations -----------------------------------------------------------------
-    def _dataterm(self, probs, verts, grad, precision, target_self=False):
+    def _dataterm(self, probs, verts, grad, precision, target_self=False, frame=True):
         """Ragged data term (lddmm_ragged_dataterm_*): NormDef values, Norm0 of
         the targets (target_self) or NormGradient w.r.t. the vertices."""
         req0 = probs[0].req
@@ -527,16 +558,33 @@ class ServingEngine(Scheduler):
         _lib.call("lddmm_ragged_dataterm_" + sfx, nreq, k, norm, vo, co, c2o, ptr(V), d, ptr(C),
                   ptr(C2) if C2 is not None else None, ptr(S2) if S2 is not None else None,
                   _f64([p.sigma_dist for p in probs]), order, 1e-10, 1e-10,
+                  _f64([c for p in probs for c in p.frame]) if (frame and self.fixed_frame) else None,
                   ptr(energy) if energy is not None else None, ptr(VP), ptr(VI),
                   ptr(px) if px is not None else None, ptr(ws), wsb, stream_handle())
         if grad:
             return [px[v_off[i]:v_off[i + 1]] for i in range(nreq)]
         return energy
 
+    def _value_precision(self):
+        return "fp64" if self.lsp == "fp64" else "fp32c"
+
     def _do_norm0(self, items):
+        """Norm0 of the targets (a constant of each request): FP64 unless the
+        line search is all-FP32c."""
         probs = [p for p, _ in items]
-        e = self._dataterm(probs, [p.v1 for p in probs], False, self.lsp, target_self=True).cpu().numpy()
+        prec = "fp32c" if self.lsp == "fp32c" else "fp64"
+        e = self._dataterm(probs, [p.v1 for p in probs], False, prec, target_self=True).cpu().numpy()
         return [float(e[i]) / p.s2 for i, p in enumerate(probs)]
+
+    def _do_refine(self, items):
+        """FP64 data term / sigmaError^2 at stored end points (the 'auto' line search)."""
+        probs = [p for p, _ in items]
+        D = self._dataterm(probs, [x for _, x in items], False, "fp64")
+        s2 = torch.tensor([p.s2 for p in probs], dtype=torch.float64, device=self.device)
+        out = (D / s2).cpu().numpy()
+        for p in probs:
+            p.calls["refine"] += 1
+        return [float(out[i]) for i in range(len(probs))]
 
     def _do_value(self, items):
         """Shooting + deformation energy (lddmm_ragged_shoot_f32c), then the data
@@ -559,12 +607,12 @@ class ServingEngine(Scheduler):
                   _f64([p.sigma_def for p in probs]), order, _f64([p.req.regweight for p in probs]), ptr(XT),
                   ptr(E), ptr(ws), wsb, stream_handle())
         xts = [XT[(T + 1) * v_off[i]:(T + 1) * v_off[i + 1]].view(T + 1, p.npt, d) for i, p in enumerate(probs)]
-        D = self._dataterm(probs, [xt[-1] for xt in xts], False, self.lsp)
+        D = self._dataterm(probs, [xt[-1] for xt in xts], False, self._value_precision())
         s2 = torch.tensor([p.s2 for p in probs], dtype=torch.float64, device=dev)
-        tot = (E + D / s2).cpu().numpy()
+        host = torch.stack([E + D / s2, E]).cpu().numpy()
         for p in probs:
             p.calls["value"] += 1
-        return [(float(tot[i]), xts[i]) for i in range(len(probs))]
+        return [(float(host[0, i]), float(host[1, i]), xts[i]) for i in range(len(probs))]
 
     def _do_grad(self, items):
         """grd.diff = (2 rw a - p_{t+1}) from the adjoint with p_T = -grad D / sigmaError^2

@@ -214,6 +214,46 @@ def test_latency_percentiles_reported():
     assert 0 < st["p50_s"] <= st["p99_s"]
 
 
+class _FakeProb:
+    def __init__(self, exact):
+        self.exact = exact
+        self.refines = 0
+
+    def exact_value(self, ereg, x_end):
+        self.refines += 1
+        return self.exact[x_end]
+
+
+def test_values_refine_only_when_the_bound_cannot_decide():
+    from registration_b200._precision import _Value as V
+    # FP32c values carry a common offset (+0.0003) that cancels in differences
+    p = _FakeProb({"a": 10.0001, "b": 10.0, "c": 12.0, "d": 10.0000005})
+    a = V(10.0004, p, 0.0, "a", 1e-3)
+    b = V(10.0003, p, 0.0, "b", 1e-3)
+    c = V(12.0003, p, 0.0, "c", 1e-3)
+    assert c > b and b < c and p.refines == 0          # |a32 - b32| > bounds: FP32c decides
+    assert a > b and p.refines == 2                     # within bounds: both refined, exact 10.0001 > 10.0
+    assert a.best == 10.0001 and a.exact and p.noise_obs < 1e-12
+    # a refined value against an unrefined one is compared on the FP32c pair
+    e = V(10.0053, p, 0.0, "c", 1e-3)
+    assert e > a and p.refines == 2
+    d = V(10.0003005, p, 0.0, "d", 1e-3)
+    # |obj - objTry| < 1e-6 test: refined to the exact 5e-7 difference
+    assert abs(d - b) < 1e-6 and p.refines == 3
+    assert 12.5 > c and c < 12.5 and float(c) == 12.0003   # plain floats on either side
+    assert 1e500 > a
+
+
+def test_value_bound_grows_with_measured_error():
+    from registration_b200._precision import _Value as V, value_bound
+    p = _FakeProb({"a": 1.0, "b": 2.0})
+    assert value_bound(p, 1e-8, 100.0) == 1e-6
+    a, b = V(1.0 + 3e-7, p, 0.0, "a", 1e-6), V(1.0 + 4e-7, p, 0.0, "b", 1e-6)
+    assert a < b            # undecided at the bound: refined, exact 1.0 < 2.0
+    assert abs(p.noise_obs - (1.0 - 1e-7)) < 1e-12
+    assert value_bound(p, 1e-8, 100.0) == 2 * p.noise_obs
+
+
 @pytest.mark.parametrize("bad", ["errorType"])
 def test_match_request_validation(bad):
     class P:
