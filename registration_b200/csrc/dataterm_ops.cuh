@@ -2,7 +2,10 @@
 // problem) and ragged.cu (many requests per launch).  Formulas and reference
 // lines: see dataterms.cu.
 #pragma once
+#include <type_traits>
+
 #include "host.h"
+#include "ops2.cuh"
 #include "pack.cuh"
 #include "sweep_dispatch.cuh"
 
@@ -121,6 +124,68 @@ struct OpData {
     }
 };
 
+// Packed-pair FP32 varifold VALUE operator (two targets per thread slot, see
+// ops2.cuh): the per-pair arithmetic of OpData<float, ..., M_VARI_VALUE>
+//   acc += K(c_k, c_l) (1 + <n_k, n_l>^2) w_l
+// with sources stored as duplicated records [y0 y1 y2 n0 n1 n2 w] (4 words)
+// and targets in the standard planes (pos word, normal word).  d = 3 only.
+template <int KIND, int PDEG>
+struct OpVariValue2 {
+    using Real = float;
+    static constexpr bool F32 = true;
+    static constexpr bool DUP = true;
+    static constexpr int TPS = 2;
+    static constexpr int BLOCK = 128, R = 4, TILE = 128, FOLD = 32;
+    static constexpr int PP = 1;
+    static constexpr int NV = 7;
+    static constexpr int NS = (NV + 1) / 2;
+    static constexpr int NOUT = 1;
+    using Params = KernelParams2;
+    using Acc = AccF32C2<1>;
+    struct Tgt {
+        f2 x[3];
+        f2 u[3];
+    };
+    struct Src {
+        f2 val[NV];
+    };
+    static LDDMM_D void load_target(const Params& P, long long ra, long long rb, Tgt& t) {
+        load_target_pair<3>(P.tgt4, P.tgt_stride, ra, rb, 0, t.x);
+        load_target_pair<3>(P.tgt4, P.tgt_stride, ra, rb, 1, t.u);
+    }
+    static LDDMM_D void load_source(const float4* S, int j, Src& s) { load_dup_source<NV, TILE>(S, j, s.val); }
+    static LDDMM_D void pair(const Params& P, const Tgt& t, const Src& s, Acc& a) {
+        f2 r2;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const f2 dj = sub2(t.x[j], s.val[j]);
+            r2 = j == 0 ? mul2(dj, dj) : fma2(dj, dj, r2);
+        }
+        const f2 k = kval2<KIND, PDEG>(P.pkd, r2);
+        const f2 dn = fma2(t.u[2], s.val[5], fma2(t.u[1], s.val[4], mul2(t.u[0], s.val[3])));
+        const f2 q = fma2(dn, dn, splat2(1.f));
+        a.fma(0, mul2(k, s.val[6]), q);
+    }
+};
+
+// Operators with duplicated source records (DUP) take duplicated polynomial
+// coefficients and a duplicated source layout from the pack.
+template <class Op, class = void>
+struct op_dup : std::false_type {};
+template <class Op>
+struct op_dup<Op, std::void_t<decltype(Op::DUP)>> : std::bool_constant<Op::DUP> {};
+
+template <class Op, class Real>
+inline void set_data_poly(typename Op::Params& P, const KScale& ks) {
+    if constexpr (op_dup<Op>::value) {
+        for (int j = 0; j < 5; ++j) P.pkd[j] = dup_coeff(ks.pk[j]);
+        for (int j = 0; j < 4; ++j) P.pqd[j] = dup_coeff(ks.pq[j]);
+    } else {
+        for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
+        for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+    }
+}
+
 // ---- geometry -----------------------------------------------------------------
 // centres (nc, d), vectors (nc, d) (surfels or tangents) of set 1; invalid cell
 // indices give zero geometry (host code validates them before the call).
@@ -174,7 +239,7 @@ LDDMM_D double vec_norm_eps(const double* s, int d, double eps) {
 template <class Real>
 LDDMM_D void dt_pack_record(int norm, int grad, bool is_t, const double* c, const double* s, int d, double eps,
                             double sign, double scale, const double* center, float4* planes, long long stride,
-                            long long i, int nplanes, int slots) {
+                            long long i, int nplanes, int slots, bool dup = false) {
     constexpr int PP = PointPlanes<Real>::N;
     if (c == nullptr) {
         for (int p = 0; p < nplanes; ++p) planes[(long long)p * stride + i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -183,6 +248,24 @@ LDDMM_D void dt_pack_record(int norm, int grad, bool is_t, const double* c, cons
     const double a = vec_norm_eps(s, d, eps);
     double pos[4] = {0, 0, 0, 0};
     for (int j = 0; j < d; ++j) pos[j] = (c[j] - center[j]) * scale;
+    if (sizeof(Real) == 4 && dup) {
+        // duplicated source record [pos0 pos1 pos2 vals...], two values per word (see ops2.cuh)
+        double vals[4] = {0, 0, 0, 0};
+        if (norm == NVARIFOLD) {
+            for (int j = 0; j < 3; ++j) vals[j] = s[j] / a;
+            vals[3] = a * sign;
+        } else if (norm == NCURRENT) {
+            for (int j = 0; j < d; ++j) vals[j] = s[j] * sign;
+        } else {
+            vals[0] = a * sign;
+        }
+        float q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int j = 0; j < 3; ++j) q[j] = (float)pos[j];
+        for (int j = 0; j < slots && j < 4; ++j) q[3 + j] = (float)vals[j];
+        for (int w = 0; w < nplanes; ++w)
+            planes[(long long)w * stride + i] = make_float4(q[2 * w], q[2 * w], q[2 * w + 1], q[2 * w + 1]);
+        return;
+    }
     if constexpr (sizeof(Real) == 4) {
         planes[i] = make_float4((float)pos[0], (float)pos[1], (float)pos[2], 0.f);
     } else {
@@ -226,7 +309,8 @@ static __global__ void dt_pack_kernel(int norm, int grad, const double* __restri
                                       long long n1, const double* __restrict__ c2, const double* __restrict__ s2,
                                       long long n2, int d, double eps1, double eps2, double sign2, double scale,
                                       const double* __restrict__ center, float4* tgt, long long tstride, int tplanes,
-                                      int tslots, float4* src, long long sstride, int splanes, int sslots) {
+                                      int tslots, float4* src, long long sstride, int splanes, int sslots,
+                                      int dup = 0) {
     const long long npad = tstride > sstride ? tstride : sstride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npad;
          i += (long long)gridDim.x * blockDim.x) {
@@ -238,7 +322,7 @@ static __global__ void dt_pack_kernel(int norm, int grad, const double* __restri
             const double* c = first ? c1 + i * d : (second ? c2 + (i - n1) * d : nullptr);
             const double* sv = first ? s1 + i * d : (second ? s2 + (i - n1) * d : nullptr);
             dt_pack_record<Real>(norm, grad, false, c, sv, d, first ? eps1 : eps2, first ? 1.0 : sign2, scale, center,
-                                 src, sstride, i, splanes, sslots);
+                                 src, sstride, i, splanes, sslots, dup != 0);
         }
     }
 }

@@ -18,6 +18,8 @@
 //
 // One sweep per call: targets = cells of set 1, sources = cells of set 1 then of
 // set 2 (target shape), both weighted per source.  No F x F array is formed.
+#include <type_traits>
+
 #include "dataterm_ops.cuh"
 #include "host.h"
 #include "pack.cuh"
@@ -58,11 +60,10 @@ int dt_sweep(const DataArgs& a, Workspace& ws, cudaStream_t st, int grad, double
     P.src_stride = pl.m_pad;
     P.tgt4 = tgt;
     P.tgt_stride = pl.n_tpad;
-    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks.pk[j];
-    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks.pq[j];
+    set_data_poly<Op, Real>(P, ks);
     dt_pack_kernel<Real><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.norm, grad, c1, s1, a.nc, a.c2, a.s2, a.nc2, a.d, a.eps1, a.eps2, sign2, ks.scale, center, tgt, pl.n_tpad,
-        Op::NT_, Op::TSLOTS, src, pl.m_pad, Op::NS, Op::SSLOTS);
+        Op::NT_, Op::TSLOTS, src, pl.m_pad, Op::NS, Op::SSLOTS, op_dup<Op>::value ? 1 : 0);
     return launch_single<Op>(pl, a.nc, P, part, st);
 }
 
@@ -94,7 +95,10 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
         int rc = LDDMM_OK;
         int nout = 1;
         if (a.norm == NVARIFOLD) {
-            using Op = DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>, 3, 4, PP + (3 + PW - 1) / PW>;
+            // FP32: packed-pair operator (two targets per slot, duplicated sources)
+            using Op = std::conditional_t<(sizeof(Real) == 4 && D == 3), DtOp<OpVariValue2<KIND, PDEG>, 3, 4, 2>,
+                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>, 3, 4,
+                                               PP + (3 + PW - 1) / PW>>;
             rc = dt_sweep<Op, Real>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else if (a.norm == NCURRENT) {

@@ -12,6 +12,7 @@
 // other requests share the launch.  Reference formulas: as the single-problem
 // entry points (pointEvolution.py:666-817, kernelFunctions.f90:1-54,
 // surfaces.py:1009-1276).
+#include <type_traits>
 #include <vector>
 
 #include "dataterm_ops.cuh"
@@ -583,7 +584,7 @@ static __global__ void rag_dt_pack_kernel(const RagSeg* __restrict__ segs, const
                                           const double* __restrict__ s1, const double* __restrict__ c2,
                                           const double* __restrict__ s2, int d, double eps1, double eps2,
                                           double sign2, float4* tgt, long long tstride, int tplanes, int tslots,
-                                          float4* src, long long sstride, int splanes, int sslots) {
+                                          float4* src, long long sstride, int splanes, int sslots, int dup) {
     const long long total = padoff[nseg];
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x) {
@@ -599,7 +600,7 @@ static __global__ void rag_dt_pack_kernel(const RagSeg* __restrict__ segs, const
             const double* c = first ? c1 + (g.row0 + i) * d : (second ? c2 + (g.m0 + i - g.n) * d : nullptr);
             const double* sv = first ? s1 + (g.row0 + i) * d : (second ? s2 + (g.m0 + i - g.n) * d : nullptr);
             dt_pack_record<Real>(norm, grad, false, c, sv, d, first ? eps1 : eps2, first ? 1.0 : sign2, g.scale,
-                                 g.center, src, sstride, g.src + i, splanes, sslots);
+                                 g.center, src, sstride, g.src + i, splanes, sslots, dup != 0);
         }
     }
 }
@@ -722,11 +723,10 @@ int rag_dt_sweep(const RagDataArgs& a, int kind, int grad, double sign2, const d
     P.tgt4 = tgt;
     P.tgt_stride = pl.tt;
     const KScale ks0 = kernel_scale<Real>(kind, a.order, a.sigma[0]);
-    for (int j = 0; j < 5; ++j) P.pk[j] = (Real)ks0.pk[j];
-    for (int j = 0; j < 4; ++j) P.pq[j] = (Real)ks0.pq[j];
+    set_data_poly<Op, Real>(P, ks0);
     rag_dt_pack_kernel<Real><<<grid_for(padoff[nseg]), 256, 0, st>>>(
         dsegs, dpad, nseg, a.norm, grad, c1, s1, a.c2, a.s2, a.d, a.eps1, a.eps2, sign2, tgt, pl.tt, NT, TSLOTS, src,
-        pl.ss, Op::NS, SSLOTS);
+        pl.ss, Op::NS, SSLOTS, op_dup<Op>::value ? 1 : 0);
     SweepGrid grid{};
     grid.segs = ddesc;
     grid.nseg = nseg;
@@ -752,7 +752,9 @@ int rag_dt_impl(const RagDataArgs& a, Workspace& ws, cudaStream_t st) {
         int nout = 1, rc = LDDMM_OK;
         long long eparts = 0;
         if (a.norm == NVARIFOLD) {
-            using Op = OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>;
+            // FP32: packed-pair operator (two targets per slot, duplicated sources)
+            using Op = std::conditional_t<(sizeof(Real) == 4 && D == 3), OpVariValue2<KIND, PDEG>,
+                                          OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>>;
             RagPlan<Op> pl;
             rc = rag_dt_sweep<Real, Op, 3, 4, PP + (3 + PW - 1) / PW>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs,
                                                                        drow, part);
