@@ -49,7 +49,12 @@ OPS = [  # name, kernel, op, flops/pair, FMA-pipe instr/pair, XU ops/pair (per-p
     ("applyK_lap3", "laplacian", "K", 24, 16, 2),
     ("applyDiffKT_lap3", "laplacian", "DKT", 28, 19, 2),
 ]
-LAUNCHES_PER_OP = {"K": 5, "DKT": 6}  # pack x2 (+1 or 2 value packs), sweep, combine
+# bounding box (init, keys, finish), target / source packs (+1 target value pack for DKT), sweep, combine
+LAUNCHES_PER_OP = {"K": 7, "DKT": 8}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one sweep launch
+# at N = M = 2^20, from one ncu capture of this workload (profiles/sweep_kernels_1M_dram.md)
+TRAFFIC_1M = {"applyK_gauss": 87339264 + 89124864, "applyDiffKT_gauss": 148929024 + 94077952,
+              "applyK_lap3": 88632576 + 84919296, "applyDiffKT_lap3": 170131712 + 133973760}
 
 
 def parse():
@@ -881,7 +886,8 @@ def main():
             per_op[o[0]] = {"ms": op_ms[o[0]], "pairs_per_s": ps_, "frac_of_measured_peak": ps_ / pk,
                             "tflops": ps_ * o[3] / 1e12}
         roof = {"bound": bound, "achieved": pairs_s / 1e9, "peak": peak_pairs / 1e9, "unit": "Gpair/s",
-                "frac": pairs_s / peak_pairs, "traffic": None, "kernel": "sweep_kernel<%s>" % dom,
+                "frac": pairs_s / peak_pairs, "traffic": TRAFFIC_1M.get(dom) if n == 1 << 20 else None,
+                "traffic_unit": "bytes per launch (ncu capture)", "kernel": "sweep_kernel<%s>" % dom,
                 "fma_instr_per_pair": opd[4], "xu_per_pair": opd[5], "flops_per_pair": opd[3],
                 "achieved_tflops": pairs_s * opd[3] / 1e12,
                 "peak_source": "measured in this run: FP32 FFMA %.3g instr/s, MUFU ex2 %.3g instr/s (probe kernels)"
