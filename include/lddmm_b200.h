@@ -213,6 +213,60 @@ LDDMM_API int lddmm_applykdiffmat_f32c(const double* x, int64_t n, const double*
 LDDMM_API int lddmm_applykdiffmat_f64(const double* x, int64_t n, const double* y, int64_t m, const double* beta,
                                       int d, double sigma, int order, double* f, lddmm_stream_t stream);
 
+/* ---- first / second derivative loops: kff.applykdiff1 ... applykdiff11and12 -----
+ * Replace py-lddmm/kernelFunctions.f90:116-496 (Kernel.applyDiffK, applyDiffK2,
+ * applyDiffK1and2, applyDDiffK11and12, kernelFunctions.py:391-455, and the
+ * dense applyDDiffK11 / applyDDiffK12, :459-507), self-interaction over x (n, d):
+ *   applykdiff1      f_k =  sum_l K' 2 <x_k-x_l, a1_k> a2_l
+ *   applykdiff2      f_k = -sum_l K' 2 <x_k-x_l, a1_l> a2_l
+ *   applykdiff1and2  f_k =  sum_l K' 2 <x_k-x_l, a1_k-a1_l> a2_l
+ *   applykdiff11     f_k =  sum_l <a1_k,a2_l> (K'' 4 <x_k-x_l, p_k> (x_k-x_l) + K' 2 p_k)
+ *   applykdiff12     f_k = -sum_l <a1_k,a2_l> (K'' 4 <x_k-x_l, p_l> (x_k-x_l) + K' 2 p_l)
+ *   applykdiff11and12 f_k = sum_l <a1_k,a2_l> (K'' 4 <dx, p_k-p_l> dx + K' 2 (p_k-p_l))
+ * a1, a2, p, f (n, d).  Order 0 is rejected; the 11 / 12 routines need a
+ * Gaussian or a Laplacian of order >= 2 (K'' table c2_).  The reference's
+ * 11 / 12 loops run over an undeclared y; these compute the intended y = x.
+ * Workspace: lddmm_applykdiffx_*_workspace(routine, n, d, order) with routine
+ * 1, 2, 3 (1and2), 11, 12, 13 (11and12). */
+LDDMM_API size_t lddmm_applykdiffx_f32c_workspace(int routine, int64_t n, int d, int order);
+LDDMM_API size_t lddmm_applykdiffx_f64_workspace(int routine, int64_t n, int d, int order);
+LDDMM_API int lddmm_applykdiff1_f32c(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                     double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                                     lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff1_f64(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                    double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                                    lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff2_f32c(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                     double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                                     lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff2_f64(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                    double sigma, int order, double* f, void* workspace, size_t workspace_bytes,
+                                    lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff1and2_f32c(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                         double sigma, int order, double* f, void* workspace,
+                                         size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff1and2_f64(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                        double sigma, int order, double* f, void* workspace,
+                                        size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff11_f32c(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                      const double* p, double sigma, int order, double* f, void* workspace,
+                                      size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff11_f64(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                     const double* p, double sigma, int order, double* f, void* workspace,
+                                     size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff12_f32c(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                      const double* p, double sigma, int order, double* f, void* workspace,
+                                      size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff12_f64(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                     const double* p, double sigma, int order, double* f, void* workspace,
+                                     size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff11and12_f32c(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                           const double* p, double sigma, int order, double* f, void* workspace,
+                                           size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_applykdiff11and12_f64(const double* x, int64_t n, int d, const double* a1, const double* a2,
+                                          const double* p, double sigma, int order, double* f, void* workspace,
+                                          size_t workspace_bytes, lddmm_stream_t stream);
+
 /* ---- ragged launches: many independent problems in one launch ----------------
  * No single counterpart in the reference (which solves one problem per process);
  * each segment computes exactly what the single-problem entry point above

@@ -56,6 +56,20 @@ SIGNATURES = {
     "lddmm_applykmat_f64": (_I, [_P, _I64, _P, _I64, _P, _I, _I, _D, _I, _P, _P]),
     "lddmm_applykdiffmat_f32c": (_I, [_P, _I64, _P, _I64, _P, _I, _D, _I, _P, _P]),
     "lddmm_applykdiffmat_f64": (_I, [_P, _I64, _P, _I64, _P, _I, _D, _I, _P, _P]),
+    "lddmm_applykdiffx_f32c_workspace": (_SZ, [_I, _I64, _I, _I]),
+    "lddmm_applykdiffx_f64_workspace": (_SZ, [_I, _I64, _I, _I]),
+    "lddmm_applykdiff1_f32c": (_I, [_P, _I64, _I, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff1_f64": (_I, [_P, _I64, _I, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff2_f32c": (_I, [_P, _I64, _I, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff2_f64": (_I, [_P, _I64, _I, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff1and2_f32c": (_I, [_P, _I64, _I, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff1and2_f64": (_I, [_P, _I64, _I, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff11_f32c": (_I, [_P, _I64, _I, _P, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff11_f64": (_I, [_P, _I64, _I, _P, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff12_f32c": (_I, [_P, _I64, _I, _P, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff12_f64": (_I, [_P, _I64, _I, _P, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff11and12_f32c": (_I, [_P, _I64, _I, _P, _P, _P, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_applykdiff11and12_f64": (_I, [_P, _I64, _I, _P, _P, _P, _D, _I, _P, _P, _SZ, _P]),
     # ragged launches: offset / sigma / regweight arguments are host arrays
     "lddmm_ragged_shoot_f32c_workspace": (_SZ, [_I, _P, _I, _I, _I]),
     "lddmm_ragged_shoot_f32c": (_I, [_I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _P, _SZ, _P]),

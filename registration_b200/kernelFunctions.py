@@ -158,6 +158,59 @@ class Kernel(KernelSpec):
             f = f * self.weight
         return output_like(x, f)
 
+    # ---- first / second derivative loops (kernelFunctions.f90:116-496) -----------
+    _KDIFF_ROUTINES = {"applykdiff1": 1, "applykdiff2": 2, "applykdiff1and2": 3, "applykdiff11": 11,
+                       "applykdiff12": 12, "applykdiff11and12": 13}
+
+    def _kdiffx(self, routine, x, a1, a2, p=None):
+        require_cuda()
+        xd, A1, A2 = to_dev(x), to_dev(a1), to_dev(a2)
+        n, d = xd.shape
+        for t in (A1, A2) + ((to_dev(p),) if p is not None else ()):
+            if tuple(t.shape) != (n, d):
+                raise ValueError("%s: a1, a2 (and p) must be (N, dim) like x" % routine)
+        if self.name == 'none':
+            return output_like(x, torch.zeros((n, d), dtype=torch.float64, device=xd.device))
+        f = torch.empty((n, d), dtype=torch.float64, device=xd.device)
+        sfx = _suffix(self.precision)
+        wsb = _lib.query("lddmm_applykdiffx_%s_workspace" % sfx, self._KDIFF_ROUTINES[routine], n, d, int(self.order))
+        ws = workspace.get(wsb)
+        args = [ptr(xd), n, d, ptr(A1.contiguous()), ptr(A2.contiguous())]
+        if p is not None:
+            args.append(ptr(to_dev(p).contiguous()))
+        _lib.call("lddmm_%s_%s" % (routine, sfx), *args, float(self.sigma), int(self.order), ptr(f), ptr(ws), wsb,
+                  stream_handle())
+        return output_like(x, f)
+
+    def applyDiffK(self, x, a1, a2):
+        """A_k = sum_l K'(x_k, x_l) 2 <x_k - x_l, a1_k> a2_l (kernelFunctions.py:391-393 -> kff.applykdiff1)."""
+        return self._kdiffx("applykdiff1", x, a1, a2)
+
+    def applyDiffK2(self, x, a1, a2):
+        """A_k = -sum_l K' 2 <x_k - x_l, a1_l> a2_l (kernelFunctions.py:396-398 -> kff.applykdiff2)."""
+        return self._kdiffx("applykdiff2", x, a1, a2)
+
+    def applyDiffK1and2(self, x, a1, a2):
+        """applyDiffK + applyDiffK2 in one sweep (kernelFunctions.py:400-402 -> kff.applykdiff1and2)."""
+        return self._kdiffx("applykdiff1and2", x, a1, a2)
+
+    def applyDDiffK11and12(self, x, n, a, p):
+        """sum_l D_11 + D_12 of n_k^T K(x_k, x_l) a_l applied to p (kernelFunctions.py:452-455 ->
+        kff.applykdiff11and12)."""
+        return self._kdiffx("applykdiff11and12", x, n, a, p)
+
+    def applyDDiffK11(self, x, n, a, p):
+        """sum_l D_11[n_k^T K(x_k, x_l) a_l] p_k (kernelFunctions.py:459-478, a dense precompute in the
+        reference, hence scaled by KernelSpec.weight; here the applykdiff11 loop)."""
+        f = self._kdiffx("applykdiff11", x, n, a, p)
+        return f * self.weight if self.weight != 1.0 else f
+
+    def applyDDiffK12(self, x, n, a, p):
+        """sum_l D_12[n_k^T K(x_k, x_l) a_l] p_l (kernelFunctions.py:481-507, dense precompute in the
+        reference, scaled by KernelSpec.weight; affine='none')."""
+        f = self._kdiffx("applykdiff12", x, n, a, p)
+        return f * self.weight if self.weight != 1.0 else f
+
     def _applykmat(self, x, a, firstVar):
         """f_k = sum_l K(y_k, x_l) a[k, l, :] with dense weights a (N_targets, N, dimb)
         (kernelFunctions.py:310-329 -> kff.applykmat, kernelFunctions.f90:499-552)."""

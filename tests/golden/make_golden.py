@@ -177,6 +177,34 @@ def kernel_cases(R, out):
     out["kernel_cases"] = np.array(cases)
 
 
+def second_cases(R, out):
+    """First / second derivative loops (kff.applykdiff1, 2, 1and2, 11and12 through
+    the reference's Kernel methods) and the reference's dense-matrix
+    applyDDiffK11 / applyDDiffK12 (kernelFunctions.py:459-507)."""
+    kf = R["kernelFunctions"]
+    rng = np.random.default_rng(777)
+    cases = []
+    for kname, order in [("gauss", 10), ("laplacian", 1), ("laplacian", 2), ("laplacian", 3), ("laplacian", 4)]:
+        for d in (2, 3):
+            n = 41
+            x = rng.uniform(0, 1, (n, d))
+            x[4] = x[3]                       # coincident points: zero-distance branch
+            a1, a2, p = (rng.standard_normal((n, d)) for _ in range(3))
+            K = kf.Kernel(name=kname, sigma=0.4, order=order)
+            tag = "%s%d_d%d" % (kname, K.order, d)
+            out["sec_x_" + tag], out["sec_a1_" + tag], out["sec_a2_" + tag], out["sec_p_" + tag] = x, a1, a2, p
+            out["sec_kd1_" + tag] = K.applyDiffK(x, a1, a2)
+            out["sec_kd2_" + tag] = K.applyDiffK2(x, a1, a2)
+            out["sec_kd12_" + tag] = K.applyDiffK1and2(x, a1, a2)
+            out["sec_r1_" + tag] = dense_kmat(R, kname, 0.4, K.order, x, x, diff=True)
+            if K.order >= 2:
+                out["sec_dd1112_" + tag] = K.applyDDiffK11and12(x, a1, a2, p)
+                out["sec_dd11_" + tag] = K.applyDDiffK11(x, a1, a2, p)
+                out["sec_dd12_" + tag] = K.applyDDiffK12(x, a1, a2, p)
+            cases.append(tag)
+    out["second_cases"] = np.array(cases)
+
+
 def evolution_cases(R, out):
     kf = R["kernelFunctions"]
     ev = R["pointEvolution"]
@@ -315,6 +343,7 @@ def main():
     R = load_reference()
     out = {}
     kernel_cases(R, out)
+    second_cases(R, out)
     evolution_cases(R, out)
     surface_cases(R, out)
     curve_cases(R, out)

@@ -147,3 +147,46 @@ def test_host_pointer_rejected_without_fault(kf):
                              ctypes.cast(arr, ctypes.c_void_p), 3, 1, 1.0, 10, ctypes.cast(arr, ctypes.c_void_p),
                              ctypes.cast(arr, ctypes.c_void_p), 4096, None)
     assert rc == -1 and b"device memory" in L.lddmm_last_error() or b"CUDA pointer" in L.lddmm_last_error()
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+def test_golden_second_derivative_loops(golden, oracle_lib, kf, precision):
+    """applyDiffK / applyDiffK2 / applyDiffK1and2 / applyDDiffK11and12 (kff loops)
+    against the reference's outputs, applyDDiffK11 / 12 against the restated
+    loops (pinned to the reference's dense matrices on the CPU)."""
+    for tag in golden["second_cases"]:
+        tag = str(tag)
+        name = "gauss" if tag.startswith("gauss") else "laplacian"
+        order = int(tag.split("_")[0].replace(name, ""))
+        x, a1, a2, p = (golden["sec_%s_%s" % (k, tag)] for k in ("x", "a1", "a2", "p"))
+        K = kf.Kernel(name=name, sigma=0.4, order=order, precision=precision)
+        assert _err(K.applyDiffK(x, a1, a2), golden["sec_kd1_" + tag]) < TOL[precision], tag
+        assert _err(K.applyDiffK2(x, a1, a2), golden["sec_kd2_" + tag]) < TOL[precision], tag
+        assert _err(K.applyDiffK1and2(x, a1, a2), golden["sec_kd12_" + tag]) < TOL[precision], tag
+        if "sec_dd11_" + tag in golden.files:
+            assert _err(K.applyDDiffK11and12(x, a1, a2, p), golden["sec_dd1112_" + tag]) < TOL[precision], tag
+            assert _err(K.applyDDiffK11(x, a1, a2, p), oracle_lib.applykdiff11(x, a1, a2, p, 0.4, order)) \
+                < TOL[precision], tag
+            assert _err(K.applyDDiffK12(x, a1, a2, p), oracle_lib.applykdiff12(x, a1, a2, p, 0.4, order)) \
+                < TOL[precision], tag
+        else:
+            with pytest.raises(ValueError):
+                K.applyDDiffK11(x, a1, a2, p)
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("name,order", [("gauss", 10), ("laplacian", 3)])
+def test_second_derivative_loops_random_sizes(oracle_lib, kf, precision, name, order):
+    rng = np.random.default_rng(order)
+    n = 3001
+    x = rng.uniform(0, 1, (n, 3))
+    a1, a2, p = (rng.standard_normal((n, 3)) for _ in range(3))
+    K = kf.Kernel(name=name, sigma=0.1, order=order, precision=precision)
+    o = K.order
+    assert _err(K.applyDiffK(x, a1, a2), oracle_lib.applykdiff1(x, a1, a2, 0.1, o)) < TOL[precision]
+    assert _err(K.applyDiffK2(x, a1, a2), oracle_lib.applykdiff2(x, a1, a2, 0.1, o)) < TOL[precision]
+    assert _err(K.applyDiffK1and2(x, a1, a2), oracle_lib.applykdiff1and2(x, a1, a2, 0.1, o)) < TOL[precision]
+    assert _err(K.applyDDiffK11(x, a1, a2, p), oracle_lib.applykdiff11(x, a1, a2, p, 0.1, o)) < TOL[precision]
+    assert _err(K.applyDDiffK12(x, a1, a2, p), oracle_lib.applykdiff12(x, a1, a2, p, 0.1, o)) < TOL[precision]
+    assert _err(K.applyDDiffK11and12(x, a1, a2, p),
+                oracle_lib.applykdiff11and12(x, a1, a2, p, 0.1, o)) < TOL[precision]

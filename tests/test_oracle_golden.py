@@ -78,6 +78,31 @@ def test_dense_weight_loops_match_reference_dense_matrices(golden, oracle_lib):
             np.testing.assert_array_equal(K.applyDiffKmat(y, b2, firstVar=x), golden["kdiffmat_f_" + tag])
 
 
+def test_second_derivative_loops_match_reference(golden, oracle_lib):
+    """kff.applykdiff1 / 2 / 1and2 / 11and12 (restated) == the reference's Kernel
+    methods on them; the restated applykdiff11 / 12 against the reference's
+    independent dense-matrix applyDDiffK11 / 12, and applykdiff1 against the
+    dense K' matrix (float32 Fortran literals: ~3e-8 for the Laplacian)."""
+    for tag in golden["second_cases"]:
+        tag = str(tag)
+        name = "gauss" if tag.startswith("gauss") else "laplacian"
+        order = int(tag.split("_")[0].replace(name, ""))
+        x, a1, a2, p = (golden["sec_%s_%s" % (k, tag)] for k in ("x", "a1", "a2", "p"))
+        tol = 1e-13 if name == "gauss" else 1e-7
+        np.testing.assert_array_equal(oracle_lib.applykdiff1(x, a1, a2, 0.4, order), golden["sec_kd1_" + tag])
+        np.testing.assert_array_equal(oracle_lib.applykdiff2(x, a1, a2, 0.4, order), golden["sec_kd2_" + tag])
+        np.testing.assert_array_equal(oracle_lib.applykdiff1and2(x, a1, a2, 0.4, order), golden["sec_kd12_" + tag])
+        dx = x[:, None, :] - x[None, :, :]
+        r1 = golden["sec_r1_" + tag]
+        dense1 = 2 * np.einsum('kl,kl,lj->kj', r1, np.einsum('kld,kd->kl', dx, a1), a2)
+        assert _rel(golden["sec_kd1_" + tag], dense1) < tol, tag
+        if "sec_dd11_" + tag in golden.files:
+            assert _rel(oracle_lib.applykdiff11(x, a1, a2, p, 0.4, order), golden["sec_dd11_" + tag]) < tol, tag
+            assert _rel(oracle_lib.applykdiff12(x, a1, a2, p, 0.4, order), golden["sec_dd12_" + tag]) < tol, tag
+            np.testing.assert_array_equal(oracle_lib.applykdiff11and12(x, a1, a2, p, 0.4, order),
+                                          golden["sec_dd1112_" + tag])
+
+
 def test_laplacian_order0_derivative_rejected(oracle_lib):
     x = np.zeros((2, 3))
     with pytest.raises(ValueError):
