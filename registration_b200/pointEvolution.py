@@ -4,6 +4,7 @@
   landmarkEPDiff               (pointEvolution.py:599-658)
   landmarkHamiltonianCovector  (pointEvolution.py:735-765)
   landmarkHamiltonianGradient  (pointEvolution.py:793-817)
+  secondOrderEvolution / Hamiltonian / Covector / Gradient (pointEvolution.py:882-1091)
 
 The plain shot and the adjoint each run as one fused C-ABI call (one kernel
 sweep + one combine per time step).  The optional outputs of the direct
@@ -151,3 +152,98 @@ def landmarkHamiltonianGradient(x0, at, px1, KparDiff, regweight, getCovector=Fa
     dA = np.zeros(np.shape(affine[0])) if not is_device(x0) else torch.zeros_like(to_dev(affine[0]))
     db = np.zeros(np.shape(affine[1])) if not is_device(x0) else torch.zeros_like(to_dev(affine[1]))
     return (dat_o, dA, db, xt_o, pxt_o) if getCovector else (dat_o, dA, db, xt_o)
+
+
+def secondOrderEvolution(x0, a0, rhot, KparDiff, withJacobian=False, withPointSet=None, affine=None):
+    """x_{k+1} = x_k + dt K(x_k) a_k,  a_{k+1} = a_k + dt (-applyDiffKT(x_k, [a_k], [a_k]) + rho_k)
+    (pointEvolution.py:882-951); returns (xt, at), or [xt, at, zt(, Jt)] with a point set.
+    The reference's withJacobian without a point set reads undefined names; it is rejected."""
+    _check_affine(affine)
+    if withJacobian and withPointSet is None:
+        raise NotImplementedError("withJacobian needs withPointSet (the reference's other branch is undefined)")
+    require_cuda()
+    x0d, a0d, rho = to_dev(x0), to_dev(a0), to_dev(rhot)
+    T = rho.shape[0]
+    dt = 1.0 / T
+    xt = torch.empty((T + 1,) + tuple(x0d.shape), dtype=torch.float64, device=x0d.device)
+    at = torch.empty_like(xt)
+    xt[0], at[0] = x0d, a0d
+    if withPointSet is not None:
+        z0 = to_dev(withPointSet)
+        zt = torch.empty((T + 1,) + tuple(z0.shape), dtype=torch.float64, device=x0d.device)
+        zt[0] = z0
+        if withJacobian:
+            Jt = torch.zeros((T + 1, z0.shape[0]), dtype=torch.float64, device=x0d.device)
+    for k in range(T):
+        x, a = xt[k], at[k]
+        zx = KparDiff.applyK(x, a)
+        za = -KparDiff.applyDiffKT(x, a[None], a[None]) + rho[k]
+        xt[k + 1] = x + dt * zx
+        at[k + 1] = a + dt * za
+        if withPointSet is not None:
+            zt[k + 1] = zt[k] + dt * KparDiff.applyK(x, a, firstVar=zt[k])
+            if withJacobian:
+                Jt[k + 1] = Jt[k] + dt * KparDiff.applyDivergence(x, a, firstVar=zt[k])
+    if withPointSet is None:
+        return output_like(x0, xt), output_like(x0, at)
+    out = [xt, at, zt] + ([Jt] if withJacobian else [])
+    return [output_like(x0, t) for t in out]
+
+
+def secondOrderHamiltonian(x, a, rho, px, pa, KparDiff, affine=None):
+    """<px, K a> + <pa, -applyDiffKT(x, [a], [a]) + rho> - |rho|^2 / 2 (pointEvolution.py:954-964)."""
+    _check_affine(affine)
+    xd, ad, rd, pxd, pad = (to_dev(v) for v in (x, a, rho, px, pa))
+    Ht = (pxd * KparDiff.applyK(xd, ad)).sum()
+    Ht = Ht + (pad * (-KparDiff.applyDiffKT(xd, ad[None], ad[None]) + rd)).sum()
+    Ht = Ht - (rd ** 2).sum() / 2
+    return float(Ht)
+
+
+def secondOrderCovector(x0, a0, rhot, px1, pa1, KparDiff, affine=None, times=None):
+    """Backward adjoint of the second-order evolution (pointEvolution.py:967-1043):
+      px_t = px_{t+1} + dt (applyDiffKT(x, [px, a], [a, px]) - applyDDiffK11and12(x, a, a, pa)),
+      pa_t = pa_{t+1} + dt (applyK(x, px) - applyDiffK1and2(x, pa, a)),
+    with the target terms px1[j], pa1[j] added at the intermediate times.  Returns
+    (pxt, pat, xt, at).  (The reference's `times=None` branch builds an unused
+    array from `range(nTarg) + 1`, which raises; it is skipped.)"""
+    _check_affine(affine)
+    require_cuda()
+    rho = to_dev(rhot)
+    T = rho.shape[0]
+    P1 = [to_dev(v) for v in px1]
+    A1 = [to_dev(v) for v in pa1]
+    nTarg = len(P1)
+    Tsize1 = T // nTarg
+    dt = 1.0 / T
+    xt, at = secondOrderEvolution(to_dev(x0), to_dev(a0), rho, KparDiff)
+    pxt = torch.zeros_like(xt)
+    pat = torch.zeros_like(xt)
+    pxt[T], pat[T] = P1[nTarg - 1], A1[nTarg - 1]
+    for t in range(T):
+        px, pa = pxt[T - t], pat[T - t]
+        x, a = xt[T - t - 1], at[T - t - 1]
+        zpx = KparDiff.applyDiffKT(x, torch.stack([px, a]), torch.stack([a, px])) \
+            - KparDiff.applyDDiffK11and12(x, a, a, pa)
+        zpa = KparDiff.applyK(x, px) - KparDiff.applyDiffK1and2(x, pa, a)
+        pxt[T - t - 1] = px + dt * zpx
+        pat[T - t - 1] = pa + dt * zpa
+        if t < T - 1 and (T - 1 - t) % Tsize1 == 0:
+            pxt[T - t - 1] += P1[(T - t - 1) // Tsize1 - 1]
+            pat[T - t - 1] += A1[(T - t - 1) // Tsize1 - 1]
+    return tuple(output_like(x0, v) for v in (pxt, pat, xt, at))
+
+
+def secondOrderGradient(x0, a0, rhot, px1, pa1, KparDiff, times=None, getCovector=False, affine=None,
+                        controlWeight=1.0):
+    """da0 = K(x0) a0 - pa_0 (pointEvolution.py:1046-1091).  Without affine the
+    reference returns drhot = 0 (its rho - pa line is commented out); kept.
+    Returns (da0, drhot, xt, at[, pxt, pat]); affine=None only."""
+    if affine is not None:
+        raise NotImplementedError("affine second-order gradients are not provided (affine=None only)")
+    pxt, pat, xt, at = secondOrderCovector(to_dev(x0), to_dev(a0), to_dev(rhot), px1, pa1, KparDiff, times=times)
+    drhot = torch.zeros_like(to_dev(rhot))
+    da0 = KparDiff.applyK(to_dev(x0), to_dev(a0)) - pat[0]
+    out = (da0, drhot, xt, at) + ((pxt, pat) if getCovector else ())
+    return tuple(output_like(x0, to_dev(v)) for v in out)
+

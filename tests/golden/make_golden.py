@@ -205,6 +205,33 @@ def second_cases(R, out):
     out["second_cases"] = np.array(cases)
 
 
+def second_order_cases(R, out):
+    """secondOrderEvolution / Hamiltonian / Covector / Gradient (pointEvolution.py:882-1091),
+    one target time (nTarg = 1) and a `times` argument (the reference's
+    times=None branch raises on `range(nTarg) + 1`)."""
+    ev = R["pointEvolution"]
+    kf = R["kernelFunctions"]
+    rng = np.random.default_rng(2468)
+    for kname, order in [("gauss", 10), ("laplacian", 3)]:
+        n, d, T = 30, 3, 5
+        x0 = rng.uniform(0, 1, (n, d))
+        a0 = 0.3 * rng.standard_normal((n, d))
+        rhot = 0.2 * rng.standard_normal((T, n, d))
+        px1 = [rng.standard_normal((n, d))]
+        pa1 = [rng.standard_normal((n, d))]
+        K = kf.Kernel(name=kname, sigma=0.5, order=order)
+        pre = "so_%s_" % kname
+        out[pre + "x0"], out[pre + "a0"], out[pre + "rhot"] = x0, a0, rhot
+        out[pre + "px1"], out[pre + "pa1"] = px1[0], pa1[0]
+        xt, at = ev.secondOrderEvolution(x0, a0, rhot, K)
+        out[pre + "xt"], out[pre + "at"] = xt, at
+        out[pre + "H"] = np.array(ev.secondOrderHamiltonian(xt[2], at[2], rhot[2], px1[0], pa1[0], K))
+        pxt, pat, _, _ = ev.secondOrderCovector(x0, a0, rhot, px1, pa1, K, times=np.ones(1))
+        out[pre + "pxt"], out[pre + "pat"] = pxt, pat
+        da0, drhot, _, _ = ev.secondOrderGradient(x0, a0, rhot, px1, pa1, K, times=np.ones(1))
+        out[pre + "da0"], out[pre + "drhot"] = da0, drhot
+
+
 def evolution_cases(R, out):
     kf = R["kernelFunctions"]
     ev = R["pointEvolution"]
@@ -344,6 +371,7 @@ def main():
     out = {}
     kernel_cases(R, out)
     second_cases(R, out)
+    second_order_cases(R, out)
     evolution_cases(R, out)
     surface_cases(R, out)
     curve_cases(R, out)

@@ -99,3 +99,28 @@ def test_epdiff_converges_to_direct_shooting(mods):
     xte, ate = ev.landmarkEPDiff(40, x0, a0, K)
     xt = ev.landmarkDirectEvolutionEuler(x0, ate, K)
     assert rel(xt[-1], xte[-1]) < 1e-6
+
+
+@pytest.mark.parametrize("kname", ["gauss", "laplacian"])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32c", 1e-5)])
+def test_second_order_evolution_covector_gradient_match_reference(golden, kname, precision, tol):
+    """secondOrderEvolution / Hamiltonian / Covector / Gradient against the
+    reference's own functions (pointEvolution.py:882-1091)."""
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import pointEvolution as evol
+    p = "so_%s_" % kname
+    K = kf.Kernel(name=kname, sigma=0.5, order=10 if kname == "gauss" else 3, precision=precision)
+    x0, a0, rhot = golden[p + "x0"], golden[p + "a0"], golden[p + "rhot"]
+    px1, pa1 = [golden[p + "px1"]], [golden[p + "pa1"]]
+
+    def close(a, b):
+        return np.abs(a - b).max() <= tol * np.abs(b).max()
+
+    xt, at = evol.secondOrderEvolution(x0, a0, rhot, K)
+    assert close(xt, golden[p + "xt"]) and close(at, golden[p + "at"])
+    H = evol.secondOrderHamiltonian(xt[2], at[2], rhot[2], px1[0], pa1[0], K)
+    assert abs(H - float(golden[p + "H"])) <= tol * abs(float(golden[p + "H"]))
+    pxt, pat, _, _ = evol.secondOrderCovector(x0, a0, rhot, px1, pa1, K)
+    assert close(pxt, golden[p + "pxt"]) and close(pat, golden[p + "pat"])
+    da0, drhot, _, _ = evol.secondOrderGradient(x0, a0, rhot, px1, pa1, K)
+    assert close(da0, golden[p + "da0"]) and np.array_equal(drhot, golden[p + "drhot"])
