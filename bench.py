@@ -80,6 +80,26 @@ def parse():
     return ap.parse_args()
 
 
+def rank_seed(seed, rank):
+    """Each rank sweeps its own seeded instance (weak scaling)."""
+    return seed + 7919 * rank
+
+
+def max_over_ranks(seconds, world, dist=None, device=None):
+    """The job's time: the slowest rank's (all ranks receive it)."""
+    if world <= 1:
+        return float(seconds)
+    import torch
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, seconds_max):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units_per_rank / seconds_max
+
+
 def make_inputs(n, seed):
     rng = np.random.default_rng(seed)
     x = rng.uniform(0, 1, (n, 3))
@@ -781,7 +801,7 @@ def main():
     from registration_b200.device import workspace
 
     n = args.n
-    x, y, a, p = make_inputs(n, args.seed + 7919 * rank)
+    x, y, a, p = make_inputs(n, rank_seed(args.seed, rank))
     xd, yd, ad, pd = (torch.from_numpy(v).to(dev) for v in (x, y, a, p))
     kernels = {"gauss": kf.Kernel(name="gauss", sigma=SIGMA), "laplacian": kf.Kernel(name="laplacian", sigma=SIGMA,
                                                                                      order=3)}
@@ -832,13 +852,9 @@ def main():
     torch.cuda.synchronize()
     step_ms = [s0.elapsed_time(s1) for s0, s1 in step_events]
     op_ms = {k: float(np.mean([e0.elapsed_time(e1) for e0, e1 in v])) for k, v in rec.items()}
-    total_s = sum(step_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([total_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
+    total_s = max_over_ranks(sum(step_ms) / 1e3, world, dist, dev)
     pairs_step = 4.0 * n * n
-    value = world * pairs_step * args.steps / total_s
+    value = job_rate(pairs_step * args.steps, world, total_s)
     ms_per_step = 1e3 * total_s / args.steps
 
     # ---- end to end through the public API with host arrays -----------------
@@ -862,12 +878,8 @@ def main():
         for op in OPS:
             r = run_op(op, kernels[op[1]], pin["x"], pin["y"], pin["a"], pin["p"])
             assert isinstance(r, np.ndarray)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * pairs_step * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dist, dev)
+    e2e_value = job_rate(pairs_step * e2e_steps, world, e2e_s)
 
     line = None
     if rank == 0:
