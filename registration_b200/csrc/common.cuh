@@ -27,7 +27,8 @@ struct SegDesc {
     int n_tb;         // target blocks
     int split;        // source chunks (one block per target block and chunk)
     int item0;        // first block index of this segment
-    int pad_;
+    int sym_tiles;    // > 0: the first sym_tiles source tiles are the targets' own records and the
+                      // sum is symmetric in (target, source): see sweep_kernel<Op, true>
 };
 
 struct SweepGrid {

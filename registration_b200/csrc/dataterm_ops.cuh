@@ -310,7 +310,9 @@ static __global__ void dt_pack_kernel(int norm, int grad, const double* __restri
                                       long long n2, int d, double eps1, double eps2, double sign2, double scale,
                                       const double* __restrict__ center, float4* tgt, long long tstride, int tplanes,
                                       int tslots, float4* src, long long sstride, int splanes, int sslots,
-                                      int dup = 0) {
+                                      int dup = 0, long long n1s = -1) {
+    // set-2 sources start at row n1s (n1 rounded up to a tile for symmetric sweeps)
+    if (n1s < 0) n1s = n1;
     const long long npad = tstride > sstride ? tstride : sstride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npad;
          i += (long long)gridDim.x * blockDim.x) {
@@ -318,9 +320,9 @@ static __global__ void dt_pack_kernel(int norm, int grad, const double* __restri
             dt_pack_record<Real>(norm, grad, true, i < n1 ? c1 + i * d : nullptr, i < n1 ? s1 + i * d : nullptr, d,
                                  eps1, 1.0, scale, center, tgt, tstride, i, tplanes, tslots);
         if (i < sstride) {
-            const bool first = i < n1, second = !first && i < n1 + n2;
-            const double* c = first ? c1 + i * d : (second ? c2 + (i - n1) * d : nullptr);
-            const double* sv = first ? s1 + i * d : (second ? s2 + (i - n1) * d : nullptr);
+            const bool first = i < n1, second = i >= n1s && i < n1s + n2;
+            const double* c = first ? c1 + i * d : (second ? c2 + (i - n1s) * d : nullptr);
+            const double* sv = first ? s1 + i * d : (second ? s2 + (i - n1s) * d : nullptr);
             dt_pack_record<Real>(norm, grad, false, c, sv, d, first ? eps1 : eps2, first ? 1.0 : sign2, scale, center,
                                  src, sstride, i, splanes, sslots, dup != 0);
         }

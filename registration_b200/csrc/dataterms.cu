@@ -47,10 +47,13 @@ struct DataArgs {
     double* px;
 };
 
-template <class Op, class Real>
+// SYM (values): the cell-cell self part is evaluated once per unordered pair
+// (sweep_kernel<Op, true>); the target cells then start at a tile boundary.
+template <class Op, class Real, bool SYM = false>
 int dt_sweep(const DataArgs& a, Workspace& ws, cudaStream_t st, int grad, double sign2, const double* c1,
              const double* s1, double*& part, SinglePlan& pl, const KScale& ks, const double* center) {
-    pl = plan_single<Op>(a.nc, a.nc + a.nc2);
+    const long long n1s = SYM ? (a.nc + Op::TILE - 1) / Op::TILE * Op::TILE : a.nc;
+    pl = plan_single<Op>(a.nc, n1s + a.nc2);
     float4* tgt = ws.take<float4>((size_t)Op::NT_ * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
     part = ws.take<double>((size_t)pl.split * a.nc * Op::NOUT);
@@ -63,8 +66,8 @@ int dt_sweep(const DataArgs& a, Workspace& ws, cudaStream_t st, int grad, double
     set_data_poly<Op, Real>(P, ks);
     dt_pack_kernel<Real><<<grid_for(std::max(pl.n_tpad, pl.m_pad)), 256, 0, st>>>(
         a.norm, grad, c1, s1, a.nc, a.c2, a.s2, a.nc2, a.d, a.eps1, a.eps2, sign2, ks.scale, center, tgt, pl.n_tpad,
-        Op::NT_, Op::TSLOTS, src, pl.m_pad, Op::NS, Op::SSLOTS, op_dup<Op>::value ? 1 : 0);
-    return launch_single<Op>(pl, a.nc, P, part, st);
+        Op::NT_, Op::TSLOTS, src, pl.m_pad, Op::NS, Op::SSLOTS, op_dup<Op>::value ? 1 : 0, n1s);
+    return launch_single<Op, SYM>(pl, a.nc, P, part, st, (int)(n1s / Op::TILE));
 }
 
 // Adapters giving OpApplyK / OpData a uniform plane description.
@@ -99,15 +102,15 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
             using Op = std::conditional_t<(sizeof(Real) == 4 && D == 3), DtOp<OpVariValue2<KIND, PDEG>, 3, 4, 2>,
                                           DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>, 3, 4,
                                                PP + (3 + PW - 1) / PW>>;
-            rc = dt_sweep<Op, Real>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
+            rc = dt_sweep<Op, Real, true>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else if (a.norm == NCURRENT) {
             using Op = DtOp<OpApplyK<Real, KIND, PDEG, D, D>, 0, D, PP>;
-            rc = dt_sweep<Op, Real>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
+            rc = dt_sweep<Op, Real, true>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else {
             using Op = DtOp<OpApplyK<Real, KIND, PDEG, D, 1>, 0, 1, PP>;
-            rc = dt_sweep<Op, Real>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
+            rc = dt_sweep<Op, Real, true>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         }
         if (rc != LDDMM_OK) return rc;

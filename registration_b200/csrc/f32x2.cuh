@@ -80,6 +80,11 @@ struct AccF32C2 {
             e[c] = add2(e[c], err);
         }
     }
+    LDDMM_D void end_fold_w(float w) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) p[c] = mul2(p[c], splat2(w));
+        end_fold();
+    }
     LDDMM_D void fma(int c, f2 a, f2 b) { p[c] = fma2(a, b, p[c]); }
     LDDMM_D double value(int c, int lane) const {
         float s0, s1, e0, e1;

@@ -584,7 +584,8 @@ static __global__ void rag_dt_pack_kernel(const RagSeg* __restrict__ segs, const
                                           const double* __restrict__ s1, const double* __restrict__ c2,
                                           const double* __restrict__ s2, int d, double eps1, double eps2,
                                           double sign2, float4* tgt, long long tstride, int tplanes, int tslots,
-                                          float4* src, long long sstride, int splanes, int sslots, int dup) {
+                                          float4* src, long long sstride, int splanes, int sslots, int dup,
+                                          int sym_align) {
     const long long total = padoff[nseg];
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x) {
@@ -596,9 +597,11 @@ static __global__ void rag_dt_pack_kernel(const RagSeg* __restrict__ segs, const
                                  i < g.n ? s1 + (g.row0 + i) * d : nullptr, d, eps1, 1.0, g.scale, g.center, tgt,
                                  tstride, g.tgt + i, tplanes, tslots);
         if (i < g.spad) {
-            const bool first = i < g.n, second = !first && i < g.n + g.m;
-            const double* c = first ? c1 + (g.row0 + i) * d : (second ? c2 + (g.m0 + i - g.n) * d : nullptr);
-            const double* sv = first ? s1 + (g.row0 + i) * d : (second ? s2 + (g.m0 + i - g.n) * d : nullptr);
+            // target-shape cells start at n rounded up to sym_align (symmetric sweeps) or at n
+            const long long n1s = sym_align > 0 ? (g.n + sym_align - 1) / sym_align * sym_align : g.n;
+            const bool first = i < g.n, second = i >= n1s && i < n1s + g.m;
+            const double* c = first ? c1 + (g.row0 + i) * d : (second ? c2 + (g.m0 + i - n1s) * d : nullptr);
+            const double* sv = first ? s1 + (g.row0 + i) * d : (second ? s2 + (g.m0 + i - n1s) * d : nullptr);
             dt_pack_record<Real>(norm, grad, false, c, sv, d, first ? eps1 : eps2, first ? 1.0 : sign2, g.scale,
                                  g.center, src, sstride, g.src + i, splanes, sslots, dup != 0);
         }
@@ -678,16 +681,20 @@ struct RagDataArgs {
     double* px;
 };
 
-template <class Real, class Op, int TSLOTS, int SSLOTS, int NT>
+// SYM (values): each segment's cell-cell self part is evaluated once per
+// unordered pair (sweep_kernel<Op, true>); its target cells start at a tile.
+template <class Real, class Op, int TSLOTS, int SSLOTS, int NT, bool SYM = false>
 int rag_dt_sweep(const RagDataArgs& a, int kind, int grad, double sign2, const double* c1, const double* s1,
                  Workspace& ws, cudaStream_t st, RagPlan<Op>& pl, RagSeg*& dsegs, long long*& drow, double*& part) {
     const int nseg = a.nseg;
-    std::vector<long long> n(nseg), m(nseg);
+    std::vector<long long> n(nseg), m(nseg), n1s(nseg);
     for (int s = 0; s < nseg; ++s) {
         n[s] = a.c_off[s + 1] - a.c_off[s];
-        m[s] = n[s] + (a.c2_off[s + 1] - a.c2_off[s]);
+        n1s[s] = SYM ? (n[s] + Op::TILE - 1) / Op::TILE * Op::TILE : n[s];
+        m[s] = n1s[s] + (a.c2_off[s + 1] - a.c2_off[s]);
     }
     pl = rag_plan<Op>(n, m);
+    for (int s = 0; s < nseg; ++s) pl.desc[s].sym_tiles = SYM ? (int)(n1s[s] / Op::TILE) : 0;
     std::vector<long long> padoff(nseg + 1, 0), rowoff(nseg + 1, 0);
     for (int s = 0; s < nseg; ++s) {
         pl.segs[s].row0 = a.c_off[s];
@@ -726,12 +733,12 @@ int rag_dt_sweep(const RagDataArgs& a, int kind, int grad, double sign2, const d
     set_data_poly<Op, Real>(P, ks0);
     rag_dt_pack_kernel<Real><<<grid_for(padoff[nseg]), 256, 0, st>>>(
         dsegs, dpad, nseg, a.norm, grad, c1, s1, a.c2, a.s2, a.d, a.eps1, a.eps2, sign2, tgt, pl.tt, NT, TSLOTS, src,
-        pl.ss, Op::NS, SSLOTS, op_dup<Op>::value ? 1 : 0);
+        pl.ss, Op::NS, SSLOTS, op_dup<Op>::value ? 1 : 0, SYM ? Op::TILE : 0);
     SweepGrid grid{};
     grid.segs = ddesc;
     grid.nseg = nseg;
     grid.n_items = pl.items;
-    if (pl.items > 0) sweep_kernel<Op><<<pl.items, Op::BLOCK, 0, st>>>(grid, P, part);
+    if (pl.items > 0) sweep_kernel<Op, SYM><<<pl.items, Op::BLOCK, 0, st>>>(grid, P, part);
     return cuda_check(cudaGetLastError(), "ragged data sweep");
 }
 
@@ -756,20 +763,20 @@ int rag_dt_impl(const RagDataArgs& a, Workspace& ws, cudaStream_t st) {
             using Op = std::conditional_t<(sizeof(Real) == 4 && D == 3), OpVariValue2<KIND, PDEG>,
                                           OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>>;
             RagPlan<Op> pl;
-            rc = rag_dt_sweep<Real, Op, 3, 4, PP + (3 + PW - 1) / PW>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs,
+            rc = rag_dt_sweep<Real, Op, 3, 4, PP + (3 + PW - 1) / PW, true>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs,
                                                                        drow, part);
             nout = Op::NOUT;
             eparts = pl.eparts;
         } else if (a.norm == NCURRENT) {
             using Op = OpApplyK<Real, KIND, PDEG, D, D>;
             RagPlan<Op> pl;
-            rc = rag_dt_sweep<Real, Op, 0, D, PP>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs, drow, part);
+            rc = rag_dt_sweep<Real, Op, 0, D, PP, true>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs, drow, part);
             nout = Op::NOUT;
             eparts = pl.eparts;
         } else {
             using Op = OpApplyK<Real, KIND, PDEG, D, 1>;
             RagPlan<Op> pl;
-            rc = rag_dt_sweep<Real, Op, 0, 1, PP>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs, drow, part);
+            rc = rag_dt_sweep<Real, Op, 0, 1, PP, true>(a, KIND, 0, -2.0, c1, s1, ws, st, pl, dsegs, drow, part);
             nout = Op::NOUT;
             eparts = pl.eparts;
         }

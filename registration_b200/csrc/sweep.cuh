@@ -11,12 +11,20 @@
 //   part[(seg.part + chunk * seg.n_tgt + t) * Op::NOUT + c]
 // and a separate combine kernel adds the chunks in a fixed order, so results
 // do not depend on scheduling.
+//
+// SYM (symmetric sums, used for energies <S,S> - 2 <S,T> whose summand is
+// symmetric in the target and the source): the first seg.sym_tiles source
+// tiles hold the targets' own records in target order.  A target block skips
+// those of its own records that precede it, counts its diagonal tiles once
+// and the later ones twice (per-tile weight applied to the FP32 fold partial,
+// exact for 1 and 2), so each unordered pair is evaluated once: the per-target
+// partial sums are no longer the per-target sums, their weighted total is.
 #pragma once
 #include "common.cuh"
 
 namespace lddmm {
 
-template <class Op>
+template <class Op, bool SYM = false>
 __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, const typename Op::Params P,
                                                            double* __restrict__ part) {
     using Real = typename Op::Real;
@@ -31,8 +39,16 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
     const int local = item - sg.item0;
     const int tb = local % sg.n_tb;
     const int chunk = local / sg.n_tb;
-    const int tile_lo = (int)(((long long)chunk * sg.n_src_tiles) / sg.split);
+    int tile_lo = (int)(((long long)chunk * sg.n_src_tiles) / sg.split);
     const int tile_hi = (int)(((long long)(chunk + 1) * sg.n_src_tiles) / sg.split);
+    int diag_hi = 0;   // SYM: own tiles at or after diag_hi (and before sym_tiles) count twice
+    if constexpr (SYM) {
+        static_assert((BLOCK * R) % TILE == 0, "symmetric sweeps need whole tiles per target block");
+        constexpr int TPB = (BLOCK * R) / TILE;
+        const int diag_lo = tb * TPB < sg.sym_tiles ? tb * TPB : sg.sym_tiles;
+        diag_hi = tb * TPB + TPB;
+        if (tile_lo < diag_lo) tile_lo = diag_lo < tile_hi ? diag_lo : tile_hi;
+    }
 
     // targets owned by this thread: t = tb*BLOCK*R + r*BLOCK + threadIdx.x (rows are padded);
     // an operator with TPS == 2 keeps two of them per slot (packed FP32 pairs)
@@ -74,6 +90,8 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
         }
         __syncthreads();
         const float4* S = smem[stage];
+        const float wt = (SYM && tile >= diag_hi && tile < sg.sym_tiles) ? 2.f : 1.f;
+        (void)wt;
 #pragma unroll 1
         for (int j0 = 0; j0 < TILE; j0 += Op::FOLD) {
 #pragma unroll
@@ -86,7 +104,10 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
                 for (int q = 0; q < SLOTS; ++q) Op::pair(P, tg[q], s, acc[q]);
             }
 #pragma unroll
-            for (int q = 0; q < SLOTS; ++q) acc[q].end_fold();
+            for (int q = 0; q < SLOTS; ++q) {
+                if constexpr (SYM) acc[q].end_fold_w(wt);
+                else acc[q].end_fold();
+            }
         }
         __syncthreads();
     }
@@ -127,6 +148,10 @@ struct AccF32C {
 #pragma unroll
         for (int c = 0; c < N; ++c) two_sum_acc(s[c], e[c], p[c]);
     }
+    LDDMM_D void end_fold_w(float w) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) two_sum_acc(s[c], e[c], p[c] * w);
+    }
     LDDMM_D void add(int c, float v) { p[c] += v; }
     LDDMM_D void fma(int c, float a, float b) { p[c] = fmaf(a, b, p[c]); }
     LDDMM_D double value(int c) const { return (double)s[c] + (double)e[c]; }
@@ -140,8 +165,17 @@ struct AccF64 {
 #pragma unroll
         for (int c = 0; c < N; ++c) s[c] = 0.0;
     }
-    LDDMM_D void begin_fold() {}
+    double m[N];   // running sum at the start of the fold (symmetric sweeps)
+    LDDMM_D void begin_fold() {
+#pragma unroll
+        for (int c = 0; c < N; ++c) m[c] = s[c];
+    }
     LDDMM_D void end_fold() {}
+    LDDMM_D void end_fold_w(float w) {
+        if (w != 1.f)
+#pragma unroll
+            for (int c = 0; c < N; ++c) s[c] = m[c] + (double)w * (s[c] - m[c]);
+    }
     LDDMM_D void add(int c, double v) { s[c] += v; }
     LDDMM_D void fma(int c, double a, double b) { s[c] = fma_rn(a, b, s[c]); }
     LDDMM_D double value(int c) const { return s[c]; }

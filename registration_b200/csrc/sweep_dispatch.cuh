@@ -37,17 +37,20 @@ SinglePlan plan_single(long long n, long long m, int split_cap = 0) {
     return p;
 }
 
-template <class Op>
-int launch_single(const SinglePlan& pl, long long n, const typename Op::Params& P, double* part, cudaStream_t st) {
+// SYM: symmetric sweep over sym_tiles own source tiles (see sweep_kernel<Op, true>)
+template <class Op, bool SYM = false>
+int launch_single(const SinglePlan& pl, long long n, const typename Op::Params& P, double* part, cudaStream_t st,
+                  int sym_tiles = 0) {
     SweepGrid g{};
     g.seg0.n_tgt = (int)n;
     g.seg0.n_src_tiles = pl.n_src_tiles;
     g.seg0.n_tb = pl.n_tb;
     g.seg0.split = pl.split;
+    g.seg0.sym_tiles = sym_tiles;
     g.nseg = 0;
     g.n_items = pl.n_tb * pl.split;
     if (g.n_items <= 0) return LDDMM_OK;
-    sweep_kernel<Op><<<g.n_items, Op::BLOCK, 0, st>>>(g, P, part);
+    sweep_kernel<Op, SYM><<<g.n_items, Op::BLOCK, 0, st>>>(g, P, part);
     return cuda_check(cudaGetLastError(), "sweep launch");
 }
 
