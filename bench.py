@@ -68,7 +68,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=16.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="kernels", choices=["kernels", "curve", "surface", "adjoint", "serving"])
+    ap.add_argument("--workload", default="kernels",
+                    choices=["kernels", "curve", "surface", "adjoint", "serving", "dataterm"])
     ap.add_argument("--iters", type=int, default=None, help="cg iterations for the matching workloads")
     ap.add_argument("--requests", type=int, default=512, help="requests of the serving stream")
     ap.add_argument("--sigma-error", type=float, default=None, help="sigmaError of the matching workloads")
@@ -774,6 +775,45 @@ def run_serving(args):
     return 0
 
 
+def run_dataterm(args):
+    """Varifold data term on a 50,000-vertex decimated icosphere (F ~ 100k cells):
+    value and gradient, FP32c and FP64, CUDA events over 5 calls after 3 warm-ups."""
+    import torch
+    from registration_b200 import _dataterm as _dt
+    from registration_b200 import geometry as geo
+    from registration_b200 import kernelFunctions as kf
+    rng = np.random.default_rng(0)
+    v, f = geo.icosphere(7)
+    v, f = geo.decimate(v, f, 50000, rng)
+    vt = geo.bumped_sphere(v, f, 10, 0.25, 0.15, rng)
+    shp = _dt.DeviceShape(f, len(v))
+    c2, s2 = _dt.cell_geometry(vt, f)
+    tc, tv = torch.from_numpy(c2).cuda(), torch.from_numpy(s2).cuda()
+    x = torch.from_numpy(v).cuda()
+    F = len(f)
+    res = {}
+    for prec in ("fp32c", "fp64"):
+        K = kf.Kernel(name="gauss", sigma=0.05, precision=prec)
+        for name, grad in (("value", False), ("gradient", True)):
+            for _ in range(max(3, args.warmup)):
+                _dt.dataterm("varifold", x, shp, tc, tv, K, energy=not grad, grad=grad)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                _dt.dataterm("varifold", x, shp, tc, tv, K, energy=not grad, grad=grad)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            res["%s_%s" % (prec, name)] = {"ms": ms, "cell_pairs_per_s": 2.0 * F * F / (ms * 1e-3)}
+    val = res["fp32c_value"]["cell_pairs_per_s"]
+    _line(args, "varifold cell pairs/s (value, F x 2F)", val, "pairs/s", True,
+          {"workload": "varifold data term, %d cells vs %d target cells, gauss sigma 0.05" % (F, F)},
+          {"ms_per_step": res["fp32c_value"]["ms"], "calls": res, "cpu_baseline": None,
+           "e2e": None})
+    return 0
+
+
 def main():
     args = parse()
     if args.workload == "curve":
@@ -784,6 +824,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "dataterm":
+        return run_dataterm(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
