@@ -168,6 +168,120 @@ struct OpVariValue2 {
     }
 };
 
+// Packed-pair FP32 varifold GRADIENT operator: the arithmetic of
+// OpData<float, ..., M_VARI_GRAD> for two target cells per slot (sources as in
+// OpVariValue2, weights carrying the -1 of the target shape):
+//   acc[0..3) += 2 <n_k,n_l> K w_l n_l,  acc[3] += K w_l (1 - <n_k,n_l>^2),
+//   acc[4..7) += K' w_l (1 + <n_k,n_l>^2) (c_k - c_l)'
+template <int KIND, int PDEG, int QDEG>
+struct OpVariGrad2 {
+    using Real = float;
+    static constexpr bool F32 = true;
+    static constexpr bool DUP = true;
+    static constexpr int TPS = 2;
+    static constexpr int BLOCK = 128, R = 2, TILE = 128, FOLD = 32;
+    static constexpr int PP = 1;
+    static constexpr int NV = 7;
+    static constexpr int NS = (NV + 1) / 2;
+    static constexpr int NOUT = 7;
+    using Params = KernelParams2;
+    using Acc = AccF32C2<NOUT>;
+    struct Tgt {
+        f2 x[3];
+        f2 u[3];
+    };
+    struct Src {
+        f2 val[NV];
+    };
+    static LDDMM_D void load_target(const Params& P, long long ra, long long rb, Tgt& t) {
+        load_target_pair<3>(P.tgt4, P.tgt_stride, ra, rb, 0, t.x);
+        load_target_pair<3>(P.tgt4, P.tgt_stride, ra, rb, 1, t.u);
+    }
+    static LDDMM_D void load_source(const float4* S, int j, Src& s) { load_dup_source<NV, TILE>(S, j, s.val); }
+    static LDDMM_D void pair(const Params& P, const Tgt& t, const Src& s, Acc& a) {
+        f2 dx[3], r2;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            dx[j] = sub2(t.x[j], s.val[j]);
+            r2 = j == 0 ? mul2(dx[j], dx[j]) : fma2(dx[j], dx[j], r2);
+        }
+        f2 k, f;
+        if constexpr (KIND == KGAUSS) {
+            k = kval2<KIND, PDEG>(P.pkd, r2);
+            f = k;
+        } else {
+            const f2 u = sqrt2(r2);
+            const f2 e = ex2neg2(u);
+            k = PDEG == 0 ? e : mul2(horner2<PDEG>(P.pkd, u), e);
+            f = QDEG == 0 ? mul2(f2{P.pqd[0]}, e) : mul2(horner2<QDEG>(P.pqd, u), e);
+        }
+        const f2 dn = fma2(t.u[2], s.val[5], fma2(t.u[1], s.val[4], mul2(t.u[0], s.val[3])));
+        const f2 wk = mul2(k, s.val[6]);
+        const f2 ca = mul2(add2(dn, dn), wk);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.fma(j, ca, s.val[3 + j]);
+        const f2 one = splat2(1.f);
+        a.fma(3, wk, fma2(mul2(dn, splat2(-1.f)), dn, one));
+        const f2 wf = mul2(mul2(f, s.val[6]), fma2(dn, dn, one));
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.fma(4 + j, wf, dx[j]);
+    }
+};
+
+// Packed-pair FP32 current GRADIENT operator (OpData<float, ..., M_CUR_GRAD>,
+// d = 3): sources [y0 y1 y2 s0 s1 s2] duplicated, targets (pos, s_k):
+//   acc[0..3) += K s_l,  acc[3..6) += K' <s_k, s_l> (c_k - c_l)'
+template <int KIND, int PDEG, int QDEG>
+struct OpCurGrad2 {
+    using Real = float;
+    static constexpr bool F32 = true;
+    static constexpr bool DUP = true;
+    static constexpr int TPS = 2;
+    static constexpr int BLOCK = 128, R = 2, TILE = 128, FOLD = 32;
+    static constexpr int PP = 1;
+    static constexpr int NV = 6;
+    static constexpr int NS = (NV + 1) / 2;
+    static constexpr int NOUT = 6;
+    using Params = KernelParams2;
+    using Acc = AccF32C2<NOUT>;
+    struct Tgt {
+        f2 x[3];
+        f2 u[3];
+    };
+    struct Src {
+        f2 val[NV];
+    };
+    static LDDMM_D void load_target(const Params& P, long long ra, long long rb, Tgt& t) {
+        load_target_pair<3>(P.tgt4, P.tgt_stride, ra, rb, 0, t.x);
+        load_target_pair<3>(P.tgt4, P.tgt_stride, ra, rb, 1, t.u);
+    }
+    static LDDMM_D void load_source(const float4* S, int j, Src& s) { load_dup_source<NV, TILE>(S, j, s.val); }
+    static LDDMM_D void pair(const Params& P, const Tgt& t, const Src& s, Acc& a) {
+        f2 dx[3], r2;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            dx[j] = sub2(t.x[j], s.val[j]);
+            r2 = j == 0 ? mul2(dx[j], dx[j]) : fma2(dx[j], dx[j], r2);
+        }
+        f2 k, f;
+        if constexpr (KIND == KGAUSS) {
+            k = kval2<KIND, PDEG>(P.pkd, r2);
+            f = k;
+        } else {
+            const f2 u = sqrt2(r2);
+            const f2 e = ex2neg2(u);
+            k = PDEG == 0 ? e : mul2(horner2<PDEG>(P.pkd, u), e);
+            f = QDEG == 0 ? mul2(f2{P.pqd[0]}, e) : mul2(horner2<QDEG>(P.pqd, u), e);
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.fma(j, k, s.val[3 + j]);
+        const f2 dot = fma2(t.u[2], s.val[5], fma2(t.u[1], s.val[4], mul2(t.u[0], s.val[3])));
+        const f2 g = mul2(f, dot);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.fma(3 + j, g, dx[j]);
+    }
+};
+
 // Operators with duplicated source records (DUP) take duplicated polynomial
 // coefficients and a duplicated source layout from the pack.
 template <class Op, class = void>

@@ -126,12 +126,17 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
         SinglePlan pl{};
         int rc = LDDMM_OK;
         int nout = 1;
+        constexpr bool PACK = sizeof(Real) == 4 && D == 3;   // FP32 surfaces: packed-pair operators
         if (a.norm == NVARIFOLD) {
-            using Op = DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_GRAD>, 3, 4, PP + (3 + PW - 1) / PW>;
+            using Op = std::conditional_t<PACK, DtOp<OpVariGrad2<KIND, PDEG, QDEG>, 3, 4, 2>,
+                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_GRAD>, 3, 4,
+                                               PP + (3 + PW - 1) / PW>>;
             rc = dt_sweep<Op, Real>(a, ws, st, 1, -1.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else if (a.norm == NCURRENT) {
-            using Op = DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_CUR_GRAD>, D, D, PP + (D + PW - 1) / PW>;
+            using Op = std::conditional_t<PACK, DtOp<OpCurGrad2<KIND, PDEG, QDEG>, D, D, 2>,
+                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_CUR_GRAD>, D, D,
+                                               PP + (D + PW - 1) / PW>>;
             rc = dt_sweep<Op, Real>(a, ws, st, 1, -1.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else {

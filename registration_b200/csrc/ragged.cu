@@ -793,14 +793,17 @@ int rag_dt_impl(const RagDataArgs& a, Workspace& ws, cudaStream_t st) {
         long long* drow = nullptr;
         double* part = nullptr;
         int nout = 1, rc = LDDMM_OK;
+        constexpr bool PACK = sizeof(Real) == 4 && D == 3;   // FP32 surfaces: packed-pair operators
         if (a.norm == NVARIFOLD) {
-            using Op = OpData<Real, KIND, PDEG, QDEG, D, M_VARI_GRAD>;
+            using Op = std::conditional_t<PACK, OpVariGrad2<KIND, PDEG, QDEG>,
+                                          OpData<Real, KIND, PDEG, QDEG, D, M_VARI_GRAD>>;
             RagPlan<Op> pl;
             rc = rag_dt_sweep<Real, Op, 3, 4, PP + (3 + PW - 1) / PW>(a, KIND, 1, -1.0, c1, s1, ws, st, pl, dsegs,
                                                                        drow, part);
             nout = Op::NOUT;
         } else if (a.norm == NCURRENT) {
-            using Op = OpData<Real, KIND, PDEG, QDEG, D, M_CUR_GRAD>;
+            using Op = std::conditional_t<PACK, OpCurGrad2<KIND, PDEG, QDEG>,
+                                          OpData<Real, KIND, PDEG, QDEG, D, M_CUR_GRAD>>;
             RagPlan<Op> pl;
             rc = rag_dt_sweep<Real, Op, D, D, PP + (D + PW - 1) / PW>(a, KIND, 1, -1.0, c1, s1, ws, st, pl, dsegs,
                                                                        drow, part);
