@@ -22,6 +22,8 @@ Other configurations (one JSON line each, not the default bench line):
     --workload adjoint  gradient of the shooting + current objective on a
                         163,842-vertex icosphere, T = 20, checkpoint every 5 steps,
                         checked against central differences in FP64
+    --workload template template estimation: 10,242-vertex hyper-template,
+                        16 bumped subjects, T = 10, 20 cg iterations
 
 Multi-GPU (torchrun): each rank sweeps its own seeded instance (weak scaling,
 no data-path collective); the time is the max over ranks.
@@ -69,7 +71,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--workload", default="kernels",
-                    choices=["kernels", "curve", "surface", "adjoint", "serving", "dataterm"])
+                    choices=["kernels", "curve", "surface", "adjoint", "serving", "dataterm", "template"])
     ap.add_argument("--iters", type=int, default=None, help="cg iterations for the matching workloads")
     ap.add_argument("--requests", type=int, default=512, help="requests of the serving stream")
     ap.add_argument("--sigma-error", type=float, default=None, help="sigmaError of the matching workloads")
@@ -436,12 +438,10 @@ def run_surface(args):
     return 0
 
 
-def surface_cpu_estimate(v, f, vt, calls, sigma_def=0.2, sigma_dist=0.1, T=10):
-    """CPU time of one match extrapolated from timed single calls of the FP64
-    C/OpenMP oracle: updateTry = shot (T applyk) + varifold value (per pair,
-    no F x F arrays), getGradient = varifold gradient + adjoint (T applykdifft),
-    dotProduct = T applyk.  The reference's own numpy varifold would build
-    F x F x 3 FP64 arrays (10 GB each at F = 20,480)."""
+def oracle_call_times(v, f, sigma_def=0.2, sigma_dist=0.1):
+    """Wall times of single FP64 C/OpenMP oracle calls on one surface (all host
+    cores): applyk (N x N), varifold value and gradient (F x 2F cell pairs,
+    computed per pair: no F x F arrays), applykdifft with na = 3 (N x N)."""
     import oracle
     oracle.build()
     oracle.set_num_threads(os.cpu_count() or 1)
@@ -464,15 +464,90 @@ def surface_cpu_estimate(v, f, vt, calls, sigma_def=0.2, sigma_dist=0.1, T=10):
     t0 = time.perf_counter()
     oracle.applykdifft(v, v, np.stack([a, a, a]), np.stack([a, a, a]), sigma_def, 10)
     t_dkt = time.perf_counter() - t0
-    per_update = T * t_k + t_val
-    per_grad = t_grad + T * t_dkt
-    per_dot = T * t_k
+    return t_k, t_val, t_grad, t_dkt
+
+
+def surface_cpu_estimate(v, f, vt, calls, sigma_def=0.2, sigma_dist=0.1, T=10, shapes=1):
+    """CPU time of one optimisation extrapolated from timed single calls of the
+    FP64 C/OpenMP oracle: updateTry = shot (T applyk) + varifold value,
+    getGradient = varifold gradient + adjoint (T applykdifft), dotProduct =
+    T applyk, each for `shapes` deformations (1 for matching; the subjects
+    + the prior for template estimation, whose prior carries no data term).
+    The reference's own numpy varifold would build F x F x 3 FP64 arrays
+    (10 GB each at F = 20,480)."""
+    t_k, t_val, t_grad, t_dkt = oracle_call_times(v, f, sigma_def, sigma_dist)
+    ndata = shapes - 1 if shapes > 1 else 1
+    per_update = shapes * T * t_k + ndata * t_val
+    per_grad = ndata * t_grad + shapes * T * t_dkt
+    per_dot = shapes * T * t_k
     total = calls["updateTry"] * per_update + calls["getGradient"] * per_grad + calls["dotProduct"] * per_dot
-    return {"value": 1.0 / total, "unit": "matches/s", "cores": os.cpu_count(), "kind": "port",
+    return {"value": 1.0 / total, "unit": "matches/s" if shapes == 1 else "templates/s", "cores": os.cpu_count(),
+            "kind": "port",
             "sample": "per-call timings of the FP64 C/OpenMP oracle (applyk %.3fs, varifold value %.3fs, "
-                      "varifold gradient %.3fs, applykdifft na=3 %.3fs) x the GPU run's call counts %s"
-                      % (t_k, t_val, t_grad, t_dkt, calls),
+                      "varifold gradient %.3fs, applykdifft na=3 %.3fs) x %d shape(s) x the GPU run's call counts %s"
+                      % (t_k, t_val, t_grad, t_dkt, shapes, calls),
             "seconds_per_match": total}
+
+
+def run_template(args):
+    """Template estimation (surfaceTemplate.py): hyper-template = icosphere
+    subdivision 5, 16 subjects with 8 seeded bumps each; cg over the prior
+    and the 16 subject deformations, the subjects' work in ragged launches."""
+    import logging
+    logging.disable(logging.INFO)
+    import torch
+    from registration_b200 import geometry as geo
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaceTemplate as ST
+    from registration_b200 import surfaces as sf
+    iters = args.iters or 20
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
+    K = 16
+    v, f = geo.icosphere(5)
+    rng = np.random.default_rng(args.seed)
+    subjects = [geo.bumped_sphere(v, f, 8, 0.25, 0.15, rng) for _ in range(K)]
+    config = {"workload": "template estimation: hyper-template icosphere %d vertices / %d faces, %d subjects (8 "
+                          "bumps each), gauss sigma 0.2, varifold sigma 0.1, sigmaError %g, lambdaPrior 1, T 10, "
+                          "%d cg iterations, TestGradient as the reference" % (len(v), len(f), K, sig_err, iters)}
+
+    def estimate(precision, maxit, lsp):
+        param = SM.SurfaceMatchingParam(timeStep=0.1,
+                                        KparDiff=kf.Kernel(name="gauss", sigma=0.2, precision=precision),
+                                        KparDist=kf.Kernel(name="gauss", sigma=0.1, precision=precision),
+                                        sigmaError=sig_err, errorType="varifold")
+        st = ST.SurfaceTemplate(HyperTmpl=sf.Surface(FV=[f, v]), Targets=[sf.Surface(FV=[f, s]) for s in subjects],
+                                param=param, maxIter=maxit, verb=False, lineSearchPrecision=lsp)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st.computeTemplate()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, st
+
+    estimate("fp32c", 2, "auto")   # warm-up
+    times = []
+    for _ in range(args.steps):
+        dt_, st = estimate("fp32c", iters, "auto")
+        times.append(dt_)
+    t_ls64, st_ls64 = estimate("fp32c", iters, "fp64")
+    t64, st64 = (None, None) if args.no_fp64 else estimate("fp64", iters, "fp64")
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = surface_cpu_estimate(v, f, None, st.calls, shapes=K + 1)
+    val = 1.0 / float(np.mean(times))
+    _line(args, "template estimations/s", val, "templates/s", True, config,
+          {"ms_per_step": 1e3 * float(np.mean(times)),
+           "ms_per_iteration": 1e3 * float(np.mean(times)) / max(1, st.iter),
+           "final_energy": float(st.obj), "iterations": st.iter, "calls": st.calls,
+           "fp32c_with_fp64_line_search": {"ms": 1e3 * t_ls64, "final_energy": float(st_ls64.obj),
+                                           "iterations": st_ls64.iter},
+           "fp64_gpu": None if st64 is None else {"ms": 1e3 * t64, "final_energy": float(st64.obj),
+                                                  "iterations": st64.iter},
+           "cpu_baseline": cpu,
+           "e2e": {"value": val, "unit": "templates/s",
+                   "h2d_bytes_per_step": int(v.nbytes * (K + 1) + f.nbytes * (K + 1)),
+                   "d2h_bytes_per_step": int(st.npt * st.dim * 8)}})
+    return 0
 
 
 def run_adjoint(args):
@@ -826,6 +901,8 @@ def main():
         return run_serving(args)
     if args.workload == "dataterm":
         return run_dataterm(args)
+    if args.workload == "template":
+        return run_template(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch

@@ -753,3 +753,188 @@ class CurveMatching(_MatchingBase):
             cg(self, verb=False, maxIter=self.maxIter, TestGradient=self.testGradient, trace=trace)
         else:
             descend(self, verb=False, maxIter=self.maxIter, trace=trace)
+
+
+# ---------------------------------------------------------------------------
+# Template estimation (py-lddmm/surfaceTemplate.py:33-369), affine 'none'
+# ---------------------------------------------------------------------------
+class TemplateDirection:
+    """surfaceTemplate.py:13-16: `prior` (T, N, d) and one Direction per subject in `all`."""
+
+    def __init__(self):
+        self.prior = []
+        self.all = []
+
+
+class SurfaceTemplate:
+    """surfaceTemplate.py:33-369 with affine='none' and no file output.
+
+    The hyper-template fv0 is deformed by the prior momenta `at` into the
+    template fvTmpl; the template is deformed by atAll[k] towards subject k.
+    Objective (surfaceTemplate.py:170-190):
+        sum_k Norm0(S_k)/s^2 + lambdaPrior E(at) + sum_k [E(atAll[k]) + NormDef(phi_k(Tmpl), S_k)/s^2].
+    The reference's SurfaceTemplate inherits objectiveFunDef from
+    SurfaceMatching but sets neither `x0` (read when no x0 is passed: the prior
+    shot) nor `v` (a per-step velocity store): the hyper-template's vertices
+    are the x0 of the prior shot here, and no velocity is stored."""
+
+    def __init__(self, HyperTmpl, Targets, param, maxIter=1000, lambdaPrior=1.0, regWeight=1.0, testGradient=True,
+                 seed=0):
+        self.fv0 = Surface(surf=HyperTmpl)
+        self.fv1 = [Surface(surf=ff) for ff in Targets]
+        self.Ntarg = len(self.fv1)
+        self.npt, self.dim = self.fv0.vertices.shape
+        self.fvTmpl = Surface(surf=self.fv0)
+        self.param = param
+        self.maxIter = maxIter
+        self.testGradient = testGradient
+        self.regweight = regWeight
+        self.lambdaPrior = lambdaPrior
+        self.Tsize = int(round(1.0 / param.timeStep))
+        shp = (self.Tsize, self.npt, self.dim)
+        self.at = np.zeros(shp)
+        self.atTry = np.zeros(shp)
+        self.xt = np.tile(self.fv0.vertices, [self.Tsize + 1, 1, 1])
+        self.atAll = [np.zeros(shp) for _ in self.fv1]
+        self.atAllTry = [np.zeros(shp) for _ in self.fv1]
+        self.xtAll = [np.tile(self.fv0.vertices, [self.Tsize + 1, 1, 1]) for _ in self.fv1]
+        self.fvDef = [Surface(surf=self.fv0) for _ in self.fv1]
+        self.tmplCoeff = 1.0
+        self.obj = None
+        self.objTry = None
+        self.gradCoeff = self.npt
+        self.iter = 0
+        self.rng = np.random.default_rng(seed)
+
+    def _obj_def(self, at, x0):
+        """objectiveFunDef (surfaceMatching.py:187-221) from x0."""
+        timeStep = 1.0 / self.Tsize
+        xt = landmarkDirectEvolutionEuler(x0, at, self.param.KparDiff)
+        obj = 0
+        for t in range(self.Tsize):
+            ra = self.param.KparDiff.applyK(xt[t], at[t])
+            obj = obj + self.regweight * timeStep * np.multiply(at[t], ra).sum()
+        return obj, xt
+
+    def _data(self, x, kk):
+        ff = Surface(surf=self.fv0)
+        ff.updateVertices(x)
+        return self.param.fun_obj(ff, self.fv1[kk], self.param.KparDist) / (self.param.sigmaError ** 2)
+
+    def objectiveFun(self):
+        """surfaceTemplate.py:170-190."""
+        if self.obj is None:
+            self.obj0 = 0
+            for fv in self.fv1:
+                self.obj0 += self.param.fun_obj0(fv, self.param.KparDist) / (self.param.sigmaError ** 2)
+            self.obj = self.obj0
+            e, self.xt = self._obj_def(self.at, self.fv0.vertices)
+            self.fvTmpl.updateVertices(self.xt[-1])
+            self.obj += e * self.lambdaPrior
+            for kk, a in enumerate(self.atAll):
+                e, xk = self._obj_def(a, self.fvTmpl.vertices)
+                self.obj += e + self._data(xk[-1], kk)
+                self.xtAll[kk] = np.copy(xk)
+        return self.obj
+
+    def getVariable(self):
+        return self.fvTmpl
+
+    def copyDir(self, dir0):
+        d = TemplateDirection()
+        d.prior = np.copy(dir0.prior)
+        for g in dir0.all:
+            d.all.append(Direction())
+            d.all[-1].diff = np.copy(g.diff)
+        return d
+
+    def randomDir(self):
+        d = TemplateDirection()
+        d.prior = self.rng.standard_normal((self.Tsize, self.npt, self.dim))
+        for _ in range(self.Ntarg):
+            d.all.append(Direction())
+            d.all[-1].diff = self.rng.standard_normal((self.Tsize, self.npt, self.dim))
+        return d
+
+    def updateTry(self, dir, eps, objRef=None):
+        """surfaceTemplate.py:215-238."""
+        objTry = self.obj0
+        atTry = self.at - eps * dir.prior
+        e, xt = self._obj_def(atTry, self.fv0.vertices)
+        objTry += e * self.lambdaPrior
+        x0 = xt[-1]
+        atAllTry = []
+        for kk, d in enumerate(dir.all):
+            atAllTry.append(self.atAll[kk] - eps * d.diff)
+            e, xk = self._obj_def(atAllTry[kk], x0)
+            objTry += e + self._data(xk[-1], kk)
+        if (objRef is None) or (objTry < objRef):
+            self.atTry = atTry
+            self.atAllTry = atAllTry
+            self.objTry = objTry
+        return objTry
+
+    def getGradient(self, coeff=1.0):
+        """surfaceTemplate.py:241-301: per subject the Hamiltonian gradient from
+        the template, its covector at t = 0 summed into the template's end-point
+        covector, then the prior's gradient from the hyper-template."""
+        pxTmpl = np.zeros((self.npt, self.dim))
+        grd = TemplateDirection()
+        for kk in range(self.Ntarg):
+            px1 = -self.param.fun_objGrad(self.fvDef[kk], self.fv1[kk], self.param.KparDist) / \
+                self.param.sigmaError ** 2
+            dat, _, pxt = landmarkHamiltonianGradient(self.fvTmpl.vertices, self.atAll[kk], px1, self.param.KparDiff,
+                                                      self.regweight, getCovector=True)
+            grd.all.append(Direction())
+            grd.all[kk].diff = dat / (coeff * self.Tsize)
+            pxTmpl += pxt[0]
+        dat, _ = landmarkHamiltonianGradient(self.fv0.vertices, self.at, pxTmpl / self.lambdaPrior,
+                                             self.param.KparDiff, self.regweight)
+        grd.prior = dat / (self.tmplCoeff * coeff * self.Tsize)
+        return grd
+
+    def dotProduct(self, g1, g2):
+        """surfaceTemplate.py:303-334."""
+        res = np.zeros(len(g2))
+        for kk, gg1 in enumerate(g1.all):
+            for t in range(self.Tsize):
+                u = self.param.KparDiff.applyK(self.xtAll[kk][t], gg1.diff[t])
+                for ll, gr in enumerate(g2):
+                    res[ll] = res[ll] + np.multiply(gr.all[kk].diff[t], u).sum()
+        for t in range(g1.prior.shape[0]):
+            u = self.param.KparDiff.applyK(self.xt[t], g1.prior[t])
+            for ll, gr in enumerate(g2):
+                res[ll] = res[ll] + np.multiply(gr.prior[t], u).sum() * (self.tmplCoeff * self.lambdaPrior)
+        return res
+
+    def acceptVarTry(self):
+        self.obj = self.objTry
+        self.at = np.copy(self.atTry)
+        for kk, a in enumerate(self.atAllTry):
+            self.atAll[kk] = np.copy(a)
+
+    def addProd(self, dir1, dir2, coeff):
+        res = TemplateDirection()
+        res.prior = dir1.prior + coeff * dir2.prior
+        for kk, dd in enumerate(dir1.all):
+            res.all.append(Direction())
+            res.all[kk].diff = dd.diff + coeff * dir2.all[kk].diff
+        return res
+
+    def endOfIteration(self):
+        """surfaceTemplate.py:353-361 without the VTK output."""
+        self.iter += 1
+        _, self.xt = self._obj_def(self.at, self.fv0.vertices)
+        self.fvTmpl.updateVertices(self.xt[-1])
+        for kk in range(self.Ntarg):
+            _, self.xtAll[kk] = self._obj_def(self.atAll[kk], self.xt[-1])
+            self.fvDef[kk].updateVertices(self.xtAll[kk][-1])
+
+    def computeTemplate(self, trace=None):
+        """surfaceTemplate.py:363-369: gradEps = max(0.1, |g|/1e4); cg with
+        TestGradient=True and the default epsInit."""
+        grd = self.getGradient(self.gradCoeff)
+        [grd2] = self.dotProduct(grd, [grd])
+        self.gradEps = max(0.1, np.sqrt(grd2) / 10000)
+        cg(self, verb=False, maxIter=self.maxIter, TestGradient=self.testGradient, trace=trace)
+        return self

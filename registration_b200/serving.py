@@ -37,7 +37,6 @@ objective is a small difference of norms of order |S|^2 / sigmaError^2.
   'fp32c': no refinement (fastest; decisions between values closer than the
       FP32c noise are arbitrary, which can end a run early).
 """
-import ctypes
 import threading
 import time
 
@@ -46,23 +45,12 @@ import torch
 
 from . import _dataterm as _dt
 from . import _lib
+from . import _ragged as _rg
 from . import conjugateGradient as cg
 from ._precision import _Value, value_bound
-from .device import ptr, require_cuda, stream_handle, workspace
+from .device import require_cuda
 
-NORMS = {"current": 0, "measure": 1, "varifold": 2}
-
-
-def _i64(a):
-    return (ctypes.c_int64 * len(a))(*[int(v) for v in a])
-
-
-def _f64(a):
-    return (ctypes.c_double * len(a))(*[float(v) for v in a])
-
-
-def _order(K):
-    return 10 if K.name == "gauss" else int(K.order)
+NORMS = _rg.NORMS
 
 
 class MatchRequest:
@@ -105,7 +93,7 @@ class MatchRequest:
     def group(self):
         """Requests of one group can share a ragged launch."""
         p = self.param
-        return (self.v0.shape[1], self.f0.shape[1], p.errorType, _order(p.KparDiff), _order(p.KparDist), self.T)
+        return (self.v0.shape[1], self.f0.shape[1], p.errorType, _rg.kernel_order(p.KparDiff), _rg.kernel_order(p.KparDist), self.T)
 
     def hbm_bytes(self):
         """Resident device state: momenta, trial momenta, gradient and three
@@ -521,49 +509,11 @@ class ServingEngine(Scheduler):
         """Ragged data term (lddmm_ragged_dataterm_*): NormDef values, Norm0 of
         the targets (target_self) or NormGradient w.r.t. the vertices."""
         req0 = probs[0].req
-        k, d = req0.f0.shape[1], req0.v0.shape[1]
-        v_off, c_off, c2_off = [0], [0], [0]
-        cells, vptr, vidx, c2, s2 = [], [], [], [], []
-        for p, v in zip(probs, verts):
-            shp = p.tshape if target_self else p.dshape
-            nc = shp.cells.shape[0]
-            cells.append(shp.cells + v_off[-1])
-            vptr.append(shp.vptr[:-1] + c_off[-1] * k)
-            vidx.append(shp.vidx + c_off[-1] * k)
-            v_off.append(v_off[-1] + v.shape[0])
-            c_off.append(c_off[-1] + nc)
-            if target_self:
-                c2_off.append(0)
-            else:
-                c2.append(p.tc)
-                s2.append(p.tv)
-                c2_off.append(c2_off[-1] + p.tc.shape[0])
-        dev = self.device
-        V = torch.cat(verts)
-        C = torch.cat(cells)
-        VP = torch.cat(vptr + [torch.full((1,), c_off[-1] * k, dtype=torch.int64, device=dev)])
-        VI = torch.cat(vidx)
-        C2 = torch.cat(c2) if c2 else None
-        S2 = torch.cat(s2) if s2 else None
-        nreq = len(probs)
-        norm = NORMS[req0.param.errorType]
-        order = _order(req0.param.KparDist)
-        sfx = "f32c" if precision == "fp32c" else "f64"
-        energy = None if grad else torch.empty(nreq, dtype=torch.float64, device=dev)
-        px = torch.empty_like(V) if grad else None
-        vo, co, c2o = _i64(v_off), _i64(c_off), _i64(c2_off)
-        wsb = _lib.query("lddmm_ragged_dataterm_%s_workspace" % sfx, nreq, k, norm, vo, co, c2o, d, order,
-                         0 if grad else 1, 1 if grad else 0)
-        ws = workspace.get(wsb)
-        _lib.call("lddmm_ragged_dataterm_" + sfx, nreq, k, norm, vo, co, c2o, ptr(V), d, ptr(C),
-                  ptr(C2) if C2 is not None else None, ptr(S2) if S2 is not None else None,
-                  _f64([p.sigma_dist for p in probs]), order, 1e-10, 1e-10,
-                  _f64([c for p in probs for c in p.frame]) if (frame and self.fixed_frame) else None,
-                  ptr(energy) if energy is not None else None, ptr(VP), ptr(VI),
-                  ptr(px) if px is not None else None, ptr(ws), wsb, stream_handle())
-        if grad:
-            return [px[v_off[i]:v_off[i + 1]] for i in range(nreq)]
-        return energy
+        return _rg.dataterm(req0.param.errorType, verts, [p.tshape if target_self else p.dshape for p in probs],
+                            None if target_self else [p.tc for p in probs],
+                            None if target_self else [p.tv for p in probs],
+                            [p.sigma_dist for p in probs], _rg.kernel_order(req0.param.KparDist), precision, grad,
+                            frames=[p.frame for p in probs] if (frame and self.fixed_frame) else None)
 
     def _value_precision(self):
         return "fp64" if self.lsp == "fp64" else "fp32c"
@@ -591,24 +541,13 @@ class ServingEngine(Scheduler):
         term at the end points: objectiveFunDef + dataTerm (surfaceMatching.py:187-231)."""
         probs = [p for p, _ in items]
         T, d = probs[0].T, probs[0].dim
-        v_off = [0]
-        for p in probs:
-            v_off.append(v_off[-1] + p.npt)
-        dev = self.device
-        X0 = torch.cat([p.x0 for p in probs])
-        AT = torch.cat([a.reshape(-1, d) for _, a in items])
-        XT = torch.empty(((T + 1) * v_off[-1], d), dtype=torch.float64, device=dev)
-        E = torch.empty(len(probs), dtype=torch.float64, device=dev)
-        vo = _i64(v_off)
-        order = _order(probs[0].req.param.KparDiff)
-        wsb = _lib.query("lddmm_ragged_shoot_f32c_workspace", len(probs), vo, d, T, order)
-        ws = workspace.get(wsb)
-        _lib.call("lddmm_ragged_shoot_f32c", len(probs), vo, d, ptr(X0), ptr(AT), T,
-                  _f64([p.sigma_def for p in probs]), order, _f64([p.req.regweight for p in probs]), ptr(XT),
-                  ptr(E), ptr(ws), wsb, stream_handle())
+        v_off = _rg.offsets([p.npt for p in probs])
+        XT, E = _rg.shoot(torch.cat([p.x0 for p in probs]), torch.cat([a.reshape(-1, d) for _, a in items]),
+                          v_off, T, [p.sigma_def for p in probs], _rg.kernel_order(probs[0].req.param.KparDiff),
+                          [p.req.regweight for p in probs])
         xts = [XT[(T + 1) * v_off[i]:(T + 1) * v_off[i + 1]].view(T + 1, p.npt, d) for i, p in enumerate(probs)]
         D = self._dataterm(probs, [xt[-1] for xt in xts], False, self._value_precision())
-        s2 = torch.tensor([p.s2 for p in probs], dtype=torch.float64, device=dev)
+        s2 = torch.tensor([p.s2 for p in probs], dtype=torch.float64, device=self.device)
         host = torch.stack([E + D / s2, E]).cpu().numpy()
         for p in probs:
             p.calls["value"] += 1
@@ -620,21 +559,12 @@ class ServingEngine(Scheduler):
         probs = [p for p, _ in items]
         T, d = probs[0].T, probs[0].dim
         pxs = self._dataterm(probs, [p.xt[-1] for p in probs], True, "fp32c")
-        v_off = [0]
-        for p in probs:
-            v_off.append(v_off[-1] + p.npt)
-        XT = torch.cat([p.xt.reshape(-1, d) for p in probs])
-        AT = torch.cat([p.at.reshape(-1, d) for p in probs])
-        PX1 = torch.cat([px / (-p.s2) for p, px in zip(probs, pxs)])
-        PXT = torch.empty_like(XT)
-        DAT = torch.empty_like(AT)
-        vo = _i64(v_off)
-        order = _order(probs[0].req.param.KparDiff)
-        wsb = _lib.query("lddmm_ragged_covector_f32c_workspace", len(probs), vo, d, T, order)
-        ws = workspace.get(wsb)
-        _lib.call("lddmm_ragged_covector_f32c", len(probs), vo, d, ptr(XT), ptr(AT), T, ptr(PX1),
-                  _f64([p.sigma_def for p in probs]), order, _f64([p.req.regweight for p in probs]), ptr(PXT),
-                  ptr(DAT), ptr(ws), wsb, stream_handle())
+        v_off = _rg.offsets([p.npt for p in probs])
+        _, DAT = _rg.covector(torch.cat([p.xt.reshape(-1, d) for p in probs]),
+                              torch.cat([p.at.reshape(-1, d) for p in probs]),
+                              torch.cat([px / (-p.s2) for p, px in zip(probs, pxs)]), v_off, T,
+                              [p.sigma_def for p in probs], _rg.kernel_order(probs[0].req.param.KparDiff),
+                              [p.req.regweight for p in probs])
         for p in probs:
             p.calls["grad"] += 1
         return [DAT[T * v_off[i]:T * v_off[i + 1]].view(T, p.npt, d) for i, p in enumerate(probs)]
@@ -654,13 +584,7 @@ class ServingEngine(Scheduler):
                 counts.append(p.npt)
                 sig.append(p.sigma_def)
             row += T * p.npt
-        U = torch.empty_like(XT)
-        st, cn = _i64(starts), _i64(counts)
-        order = _order(probs[0].req.param.KparDiff)
-        wsb = _lib.query("lddmm_ragged_applyk_f32c_workspace", len(starts), cn, cn, d, d, order)
-        ws = workspace.get(wsb)
-        _lib.call("lddmm_ragged_applyk_f32c", len(starts), st, cn, st, cn, d, ptr(XT), ptr(XT), ptr(G1), d,
-                  _f64(sig), order, ptr(U), ptr(ws), wsb, stream_handle())
+        U = _rg.applyk_segments(XT, G1, starts, counts, sig, _rg.kernel_order(probs[0].req.param.KparDiff))
         outs = []
         row = 0
         for p, (_, g2s) in items:
@@ -675,6 +599,7 @@ class ServingEngine(Scheduler):
             res.append(host[k:k + len(g2s)].copy())
             k += len(g2s)
         return res
+
 
 def serve(requests, **engine_kw):
     """Runs a list of requests (arrival times already set, or now) to completion."""

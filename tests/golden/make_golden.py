@@ -64,7 +64,7 @@ def _py3_source(text):
 
 def load_reference(names=("kernelFunctions", "affineBasis", "pointEvolution", "surfaces", "curves",
                            "matchingParam", "grid", "conjugateGradient", "gradientDescent", "surfaceMatching",
-                           "curveMatching")):
+                           "curveMatching", "surfaceTemplate")):
     sys.modules["kernelFunctions_fort"] = oracle.FortShim()
     sys.modules["gaussianDiffeons"] = types.ModuleType("gaussianDiffeons")
     mods = {}
@@ -364,6 +364,42 @@ def matching_cases(R, out):
         out[p + "gradEps"] = cm.gradEps
 
 
+def template_cases(R, out):
+    """Template estimation (surfaceTemplate.py) on three bumped icospheres.  The
+    reference's SurfaceTemplate never sets two attributes that the inherited
+    SurfaceMatching.objectiveFunDef reads (x0, used by the prior's shot, and
+    the velocity store v); they are set on the instance to the hyper-template's
+    vertices and a zero store before the run."""
+    kf = R["kernelFunctions"]
+    sf = R["surfaces"]
+    SM = R["surfaceMatching"]
+    ST = R["surfaceTemplate"]
+    tmp = tempfile.mkdtemp(prefix="lddmm_golden_")
+    rng = np.random.default_rng(11)
+    v, f = geo.icosphere(2)
+    subjects = [geo.bumped_sphere(v, f, 5, 0.4, 0.2, rng) for _ in range(3)]
+    out["st_faces"] = f
+    out["st_v0"] = v
+    out["st_subjects"] = np.stack(subjects)
+    for err, lam in [("varifold", 1.0), ("current", 0.5)]:
+        param = SM.SurfaceMatchingParam(timeStep=0.2, KparDiff=kf.Kernel(name="gauss", sigma=0.4),
+                                        KparDist=kf.Kernel(name="gauss", sigma=0.3), sigmaError=0.1,
+                                        errorType=err)
+        st = ST.SurfaceTemplate(HyperTmpl=sf.Surface(FV=[f, v]), Targets=[sf.Surface(FV=[f, s]) for s in subjects],
+                                param=param, maxIter=5, lambdaPrior=lam, verb=False, outputDir=tmp)
+        st.x0 = np.copy(st.fv0.vertices)
+        st.v = np.zeros((st.Tsize, st.npt, st.dim))
+        trace = _record_trace(st)
+        np.random.seed(7)      # cg's TestGradient direction (logged only)
+        st.computeTemplate()
+        p = "st_%s_" % err
+        out[p + "trace"] = np.array([float(st.obj0)] + trace)
+        out[p + "at"] = np.copy(st.at)
+        out[p + "atAll"] = np.stack(st.atAll)
+        out[p + "gradEps"] = st.gradEps
+        out[p + "tmpl"] = np.copy(st.fvTmpl.vertices)
+
+
 def main():
     oracle.build()
     oracle.set_num_threads(4)
@@ -376,6 +412,7 @@ def main():
     surface_cases(R, out)
     curve_cases(R, out)
     matching_cases(R, out)
+    template_cases(R, out)
     dst = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(dst, **out)
     print("wrote %s (%d arrays, %.1f KB)" % (dst, len(out), os.path.getsize(dst) / 1024.0))

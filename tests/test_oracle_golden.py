@@ -186,3 +186,22 @@ def test_curve_matching_trace_matches_reference(golden, oracle_lib, err):
     p = "cm_%s_" % err
     np.testing.assert_allclose([cm.obj0] + trace, golden[p + "trace"], rtol=1e-9)
     np.testing.assert_allclose(cm.at, golden[p + "at"], rtol=1e-7, atol=1e-10)
+
+
+@pytest.mark.parametrize("err,lam", [("varifold", 1.0), ("current", 0.5)])
+def test_template_estimation_trace_matches_reference(golden, oracle_lib, err, lam):
+    """surfaceTemplate.py (cg over the prior and three subjects) against the
+    reference's own SurfaceTemplate run on the same shapes."""
+    f, v0, subs = golden["st_faces"], golden["st_v0"], golden["st_subjects"]
+    param = ref.MatchingParam(timeStep=0.2, KparDiff=ref.Kernel(name="gauss", sigma=0.4),
+                              KparDist=ref.Kernel(name="gauss", sigma=0.3), sigmaError=0.1, errorType=err)
+    st = ref.SurfaceTemplate(ref.Surface(FV=[f, v0]), [ref.Surface(FV=[f, s]) for s in subs], param, maxIter=5,
+                             lambdaPrior=lam, testGradient=False)
+    trace = []
+    st.computeTemplate(trace=trace)
+    p = "st_%s_" % err
+    assert st.gradEps == golden[p + "gradEps"]
+    np.testing.assert_allclose([st.obj0] + trace, golden[p + "trace"], rtol=1e-9)
+    np.testing.assert_allclose(st.at, golden[p + "at"], rtol=1e-7, atol=1e-10)
+    np.testing.assert_allclose(np.stack(st.atAll), golden[p + "atAll"], rtol=1e-7, atol=1e-10)
+    np.testing.assert_allclose(st.fvTmpl.vertices, golden[p + "tmpl"], rtol=1e-9, atol=1e-12)
