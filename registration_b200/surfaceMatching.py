@@ -49,8 +49,14 @@ class SurfaceMatching(DeviceMatching):
                  regWeight=1.0, affineWeight=1.0, verb=True, subsampleTargetSize=-1, rotWeight=None,
                  scaleWeight=None, transWeight=None, symmetric=False, testGradient=True, saveFile='evolution',
                  affine='none', outputDir='.', lineSearchPrecision='fp64'):
-        if Template is None or Target is None:
-            raise ValueError('Please provide template and target surfaces (file readers are not provided)')
+        if Template is None:
+            if fileTempl is None:
+                raise ValueError('Please provide a template surface')
+            Template = surfaces.Surface(filename=fileTempl)
+        if Target is None:
+            if fileTarg is None:
+                raise ValueError('Please provide a target surface')
+            Target = surfaces.Surface(filename=fileTarg)
         if subsampleTargetSize > 0:
             raise NotImplementedError('template simplification (VTK) is not provided')
         self.fv0 = surfaces.Surface(surf=Template)

@@ -68,8 +68,14 @@ class SurfaceTemplate:
                  transWeight=None, testGradient=False, saveFile='evolution', affine='none', outputDir='.',
                  lineSearchPrecision='fp64', noise=1e-8):
         require_cuda()
-        if HyperTmpl is None or Targets is None:
-            raise ValueError('Please provide a hyper-template and target surfaces (file readers are not provided)')
+        if HyperTmpl is None:
+            if fileHTempl is None:
+                raise ValueError('Please provide a hyper-template surface')
+            HyperTmpl = surfaces.Surface(filename=fileHTempl)
+        if Targets is None:
+            if fileTarg is None:
+                raise ValueError('Please provide target surfaces')
+            Targets = [surfaces.Surface(filename=ff) for ff in fileTarg]
         if affine not in ('none', None):
             raise NotImplementedError("affine registration components are not provided (affine='none' only)")
         if lineSearchPrecision not in ('fp64', 'auto', 'fp32c'):

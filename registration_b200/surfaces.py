@@ -3,7 +3,9 @@ py-lddmm/surfaces.py, computed on the GPU.
 
   Surface(surf=None, filename=None, FV=None)     surfaces.py:24-75
     .vertices, .faces, .centers, .surfel, computeCentersAreas(), updateVertices(x),
-    flipFaces(), surfVolume(), saveVTK(fileName)
+    flipFaces(), surfVolume(), readbyu / readOFF / readVTK / readOBJ, savebyu, saveVTK / saveVTK2,
+    computeVertexArea(), computeVertexNormals()                               surfaces.py:77-139, 711-985
+  readMultipleByu, saveEvolution, vtkFields, readskip                          surfaces.py:16-21, 988-1005, 1279
   currentNorm0 / currentNormDef / currentNormGradient      surfaces.py:1009-1089
   measureNorm0 / measureNormDef / measureNormGradient      surfaces.py:1092-1182
   varifoldNorm0 / varifoldNormDef / varifoldNormGradient   surfaces.py:1184-1276
@@ -12,14 +14,18 @@ py-lddmm/surfaces.py, computed on the GPU.
 The norms take the same arguments as the reference (fvDef, fv1, KparDist) and
 return a float (value) or an (nv, 3) float64 array (gradient; a CUDA tensor
 when the surface holds device vertices).  None of them forms an F x F array.
-Reading meshes from .byu/.off/.vtk/.obj files (VTK) is not part of this library.
+Mesh files (.byu / .off / legacy ASCII .vtk / .obj), vertex areas and vertex
+normals: registration_b200.meshio (host side).
 """
+import glob
+import logging
 import os
 
 import numpy as np
 import torch
 
 from . import _dataterm as _dt
+from . import meshio
 
 
 class Surface:
@@ -33,7 +39,18 @@ class Surface:
             self.faces = np.int_(np.asarray(FV[0]))
             self._dshape = None
         elif filename is not None:
-            raise NotImplementedError("mesh file readers are not part of this library; build Surface(FV=[faces, v])")
+            self._dshape = None
+            ext = os.path.splitext(filename)[1]
+            readers = {'.byu': self.readbyu, '.off': self.readOFF, '.vtk': self.readVTK, '.obj': self.readOBJ}
+            if ext not in readers:
+                logging.error('Unknown Surface Extension: %s', ext)
+                self.vertices = np.empty(0)
+                self.faces = np.empty(0, dtype=np.int64)
+                self.centers = np.empty(0)
+                self.surfel = np.empty(0)
+                return
+            readers[ext](filename)
+            return
         else:
             self.vertices = np.empty(0)
             self.faces = np.empty(0, dtype=np.int64)
@@ -68,26 +85,82 @@ class Surface:
             self._dshape = _dt.DeviceShape(self.faces, len(self.vertices))
         return self._dshape
 
-    def saveVTK(self, fileName, scalars=None, normals=None, scal_name='scalars'):
-        """ASCII legacy VTK polydata (points and triangles, optional point scalars)."""
-        V = _np(self.vertices)
-        F = self.faces
+    def _set_mesh(self, vertices, faces):
+        self.vertices = vertices
+        self.faces = np.int_(faces)
+        self._dshape = None
+        self.computeCentersAreas()
+
+    # -- files (surfaces.py:719-985) -------------------------------------------------------
+    def readbyu(self, byufile):
+        """(surfaces.py:757-805)"""
+        self._set_mesh(*meshio.read_byu(byufile))
+
+    def readOFF(self, offfile):
+        """(surfaces.py:719-754)"""
+        self._set_mesh(*meshio.read_off(offfile))
+
+    def readVTK(self, fileName):
+        """legacy ASCII POLYDATA (the reference reads it through VTK, surfaces.py:928-955)"""
+        self._set_mesh(*meshio.read_vtk(fileName))
+
+    def readOBJ(self, fileName):
+        """(the reference reads it through VTK, surfaces.py:957-985)"""
+        self._set_mesh(*meshio.read_obj(fileName))
+
+    def savebyu(self, byufile):
+        """(surfaces.py:807-849)"""
+        meshio.write_byu(byufile, _np(self.vertices), self.faces)
+
+    def saveVTK(self, fileName, scalars=None, normals=None, tensors=None, scal_name='scalars', vectors=None,
+                vect_name='vectors'):
+        """(surfaces.py:851-867)"""
+        vf = meshio.vtkFields()
+        if scalars is not None:
+            vf.scalars += [scal_name, _np(scalars)]
+        if vectors is not None:
+            vf.vectors += [vect_name, _np(vectors)]
+        if normals is not None:
+            vf.normals += ['normals', _np(normals)]
+        if tensors is not None:
+            vf.tensors += ['tensors', _np(tensors)]
+        self.saveVTK2(fileName, vf)
+
+    def saveVTK2(self, fileName, vtkFields=None):
+        """(surfaces.py:869-925)"""
         d = os.path.dirname(fileName)
         if d:
             os.makedirs(d, exist_ok=True)
-        with open(fileName, 'w') as fh:
-            fh.write('# vtk DataFile Version 3.0\nSurface Data\nASCII\nDATASET POLYDATA\n')
-            fh.write('\nPOINTS {0:d} float'.format(V.shape[0]))
-            for p in V:
-                fh.write('\n{0: f} {1: f} {2: f}'.format(p[0], p[1], p[2]))
-            fh.write('\nPOLYGONS {0:d} {1:d}'.format(F.shape[0], 4 * F.shape[0]))
-            for f in F:
-                fh.write('\n3 {0:d} {1:d} {2:d}'.format(f[0], f[1], f[2]))
-            if scalars is not None:
-                fh.write('\nPOINT_DATA {0:d}\nSCALARS {1} float 1\nLOOKUP_TABLE default'.format(V.shape[0], scal_name))
-                for s in np.asarray(scalars):
-                    fh.write('\n {0: .5f}'.format(s))
-            fh.write('\n')
+        meshio.write_vtk(fileName, _np(self.vertices), self.faces, vtkFields)
+
+    # -- per-vertex geometry (surfaces.py:77-139) ------------------------------------------------
+    def computeVertexArea(self):
+        """(AV (nv, 1), AF (nf, 1)) (surfaces.py:77-126)"""
+        return meshio.vertex_area(_np(self.vertices), self.faces)
+
+    def computeVertexNormals(self):
+        """(surfaces.py:128-139)"""
+        self.computeCentersAreas()
+        return meshio.vertex_normals(_np(self.vertices), self.faces)
+
+
+def readMultipleByu(regexp, Nmax=0):
+    """Surfaces of the .byu files matching a glob pattern (surfaces.py:988-997)."""
+    files = glob.glob(regexp)
+    nm = min(Nmax, len(files)) if Nmax > 0 else len(files)
+    return [Surface(filename=files[k]) for k in range(nm)]
+
+
+def saveEvolution(fileName, fv0, xt):
+    """One .byu file per time step of a trajectory xt (T+1, N, 3) (surfaces.py:1000-1005)."""
+    fv = Surface(surf=fv0)
+    xt = _np(xt)
+    for k in range(xt.shape[0]):
+        meshio.write_byu(fileName + '{0: 02d}'.format(k) + '.byu', xt[k], fv.faces)
+
+
+vtkFields = meshio.vtkFields
+readskip = meshio.readskip
 
 
 def _copy(x):

@@ -5,7 +5,7 @@ f2py Fortran module.  In this container there is neither a Python 2
 interpreter nor a Fortran compiler, so this script:
 
 1. loads the reference's own Python modules from the read-only checkout
-   (default /root/reference/py-lddmm, or $LDDMM_REFERENCE_DIR) after three
+   (default /root/reference/py-lddmm, or $LDDMM_REFERENCE_DIR) after four
    mechanical, semantics-preserving source rewrites done in memory
    (nothing is copied into this repository):
      - tabs expanded to 8-column stops (Python 2 indentation rule);
@@ -13,6 +13,7 @@ interpreter nor a Fortran compiler, so this script:
      - ``== None`` / ``!= None`` turned into ``is None`` / ``is not None``
        (what the comparison returned for arrays under the numpy of the
        Python 2 era; modern numpy compares element-wise instead);
+     - ``len(x)/2`` turned into ``len(x)//2`` (Python 2 integer division);
 2. registers the oracle (``oracle.FortShim``, a C/OpenMP restatement of
    kernelFunctions.f90) as the module ``kernelFunctions_fort`` that the
    reference imports, and a stub ``gaussianDiffeons`` (imported by
@@ -58,6 +59,7 @@ def _py3_source(text):
             line = "%sprint(%s)" % (m.group(1), body.rstrip(","))
         line = re.sub(r"!=\s*None\b", " is not None", line)
         line = re.sub(r"==\s*None\b", " is None", line)
+        line = re.sub(r"(len\([^()]*\))/2\b", r"\1//2", line)
         out.append(line)
     return "\n".join(out) + "\n"
 
@@ -77,8 +79,8 @@ def load_reference(names=("kernelFunctions", "affineBasis", "pointEvolution", "s
         sys.modules[nm] = mod
         exec(compile(src, path, "exec"), mod.__dict__)
         mods[nm] = mod
-    # output-only writers -> no-ops
-    mods["surfaces"].Surface.saveVTK = lambda self, *a, **k: None
+    # output-only writers -> no-ops (the VTK writer itself is kept for the mesh cases)
+    mods["surfaces_saveVTK2"] = mods["surfaces"].Surface.saveVTK2
     mods["surfaces"].Surface.saveVTK2 = lambda self, *a, **k: None
     mods["curves"].Curve.saveVTK = lambda self, *a, **k: None
     mods["grid"].Grid.saveVTK = lambda self, *a, **k: None
@@ -400,6 +402,51 @@ def template_cases(R, out):
         out[p + "tmpl"] = np.copy(st.fvTmpl.vertices)
 
 
+def mesh_cases(R, out):
+    """Mesh files and per-vertex geometry (surfaces.py:77-139, 711-925) on a
+    perturbed, decimated icosphere (obtuse faces, odd vertex count).  The
+    reference's readbyu calls scipy.fabs, one of the numpy functions that
+    scipy re-exported in the Python 2 era; numpy's fabs is bound in its
+    place for the run."""
+    sf = R["surfaces"]
+    sf.sp = types.SimpleNamespace(fabs=np.fabs)
+    tmp = tempfile.mkdtemp(prefix="lddmm_golden_")
+    rng = np.random.default_rng(21)
+    v, f = geo.icosphere(3)
+    v, f = geo.decimate(v + 0.02 * rng.standard_normal(v.shape), f, 301, rng)
+    out["mesh_v"] = v
+    out["mesh_f"] = f
+    fv = sf.Surface(FV=[f, v])
+    AV, AF = fv.computeVertexArea()
+    out["mesh_AV"] = AV
+    out["mesh_AF"] = AF
+    out["mesh_normals"] = fv.computeVertexNormals()
+    out["mesh_volume"] = fv.surfVolume()
+    byu = os.path.join(tmp, "m.byu")
+    fv.savebyu(byu)
+    with open(byu) as fh:
+        out["mesh_byu_text"] = np.array(fh.read())
+    back = sf.Surface(filename=byu)
+    out["mesh_byu_v"] = back.vertices
+    out["mesh_byu_f"] = back.faces
+    vtk = os.path.join(tmp, "m.vtk")
+    sf.Surface.saveVTK2 = R["surfaces_saveVTK2"]
+    fv.saveVTK(vtk, scalars=AV[:, 0], normals=out["mesh_normals"], vectors=0.5 * out["mesh_normals"])
+    sf.Surface.saveVTK2 = lambda self, *a, **k: None
+    with open(vtk) as fh:
+        out["mesh_vtk_text"] = np.array(fh.read())
+    off_lines = ["# written for the golden fixtures", "OFF", "# counts", "%d %d 0" % (len(v), len(f))]
+    off_lines += ["%.17g %.17g %.17g" % tuple(p) for p in v]
+    off_lines += ["# faces"] + ["3 %d %d %d" % tuple(t) for t in f]
+    off = os.path.join(tmp, "m.off")
+    with open(off, "w") as fh:
+        fh.write("\n".join(off_lines) + "\n")
+    out["mesh_off_text"] = np.array("\n".join(off_lines) + "\n")
+    back = sf.Surface(filename=off)
+    out["mesh_off_v"] = back.vertices
+    out["mesh_off_f"] = back.faces
+
+
 def main():
     oracle.build()
     oracle.set_num_threads(4)
@@ -413,6 +460,7 @@ def main():
     curve_cases(R, out)
     matching_cases(R, out)
     template_cases(R, out)
+    mesh_cases(R, out)
     dst = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(dst, **out)
     print("wrote %s (%d arrays, %.1f KB)" % (dst, len(out), os.path.getsize(dst) / 1024.0))

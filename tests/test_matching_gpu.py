@@ -92,3 +92,26 @@ def test_user_plugged_data_term_is_honoured(golden):
     sm.optimizeMatching()
     logging.disable(logging.NOTSET)
     assert calls["n"] > 0
+
+
+def test_matching_from_mesh_files(golden, tmp_path):
+    """fileTempl / fileTarg (surfaceMatching.py:83-97) read .byu / .vtk files."""
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import meshio
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+    f, v0, v1 = golden["sm_faces"], golden["sm_v0"], golden["sm_v1"]
+    p0, p1 = str(tmp_path / "t.byu"), str(tmp_path / "s.vtk")
+    sf.Surface(FV=[f, v0]).savebyu(p0)
+    sf.Surface(FV=[f, v1]).saveVTK(p1)
+    param = SM.SurfaceMatchingParam(timeStep=0.2, KparDiff=kf.Kernel(name="gauss", sigma=0.4),
+                                    KparDist=kf.Kernel(name="gauss", sigma=0.3), sigmaError=0.5, errorType="varifold")
+    a = SM.SurfaceMatching(fileTempl=p0, fileTarg=p1, param=param, maxIter=2, testGradient=False)
+    va, fa = meshio.read_byu(p0)
+    vb, fb = meshio.read_vtk(p1)
+    b = SM.SurfaceMatching(Template=sf.Surface(FV=[fa, va]), Target=sf.Surface(FV=[fb, vb]), param=param, maxIter=2,
+                           testGradient=False)
+    a.optimizeMatching()
+    b.optimizeMatching()
+    assert float(a.obj) == float(b.obj)
+    assert bool((a.at == b.at).all())
