@@ -1,6 +1,6 @@
 """GPU parity of the kernel sums (applyK / applyDiffKT) against the oracle.
 
-Tolerances (north-star accuracy bar):
+Tolerances (the accuracy bar of the FP32 compensated path):
   fp32c: relative error <= 1e-5 against the FP64 oracle, measured as
          ||f - f_ref||_F / ||f_ref||_F and max_k ||f_k - f_ref_k|| / max_k ||f_ref_k||;
   fp64 : the same two measures <= 1e-12.
