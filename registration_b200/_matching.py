@@ -32,7 +32,7 @@ import torch
 from . import _dataterm as _dt
 from . import pointEvolution as evol
 from ._precision import _Value, value_bound
-from .device import require_cuda, to_dev
+from .device import require_cuda, to_dev, workspace
 
 
 class Direction:
@@ -46,7 +46,7 @@ class DeviceMatching:
     """Subclasses set: fv0, fv1 (shapes), param, norm_name, tgt_vectors_attr."""
 
     def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision='fp64',
-                    noise=1e-8):
+                    noise=1e-8, cudaGraphs=True):
         require_cuda()
         if affine not in ('none', None):
             raise NotImplementedError("affine registration components are not provided (affine='none' only)")
@@ -71,6 +71,8 @@ class DeviceMatching:
         self.xt = self.x0.unsqueeze(0).repeat(self.Tsize + 1, 1, 1)
         self.xtTry = None
         self.calls = {"updateTry": 0, "getGradient": 0, "dotProduct": 0}
+        self.cudaGraphs = bool(cudaGraphs)
+        self._graph = None
         self.obj = None
         self.objTry = None
         self.gradCoeff = self.npt
@@ -168,6 +170,8 @@ class DeviceMatching:
     def updateTry(self, dir, eps, objRef=None):
         """(surfaceMatching.py:255-289); NaN objectives return 1e500."""
         self.calls["updateTry"] += 1
+        if self.cudaGraphs and self._fast_data:
+            return self._graph_update_try(dir, eps, objRef)
         atTry = self.at - eps * dir.diff
         xt, e = evol.shoot(self.x0, atTry, self.param.KparDiff, regweight=self.regweight, with_energy=True)
         objTry = self._trial_value(e, xt[-1])
@@ -178,6 +182,56 @@ class DeviceMatching:
             self.atTry = atTry
             self.objTry = objTry
             self.xtTry = xt
+        return objTry
+
+    # -- the trial step as one CUDA graph --------------------------------------------------
+    def _trial_body(self):
+        """atTry = at - eps dir, its shot and its data-term value, on static buffers."""
+        g = self._graph
+        torch.sub(g["at"], torch.mul(g["dir"], g["eps"]), out=g["atTry"])
+        xt, e = evol.shoot(self.x0, g["atTry"], self.param.KparDiff, regweight=self.regweight, with_energy=True)
+        return xt, torch.stack([e, self._data_energy(xt[-1])])
+
+    def _graph_update_try(self, dir, eps, objRef):
+        """updateTry with the shot and the data-term value replayed from a CUDA
+        graph captured on the first call: the same kernels on the same inputs
+        (bit-identical to the eager path), one launch from the host, one read
+        back.  The static copies of `at` and of the direction are refreshed
+        only when cg hands over new tensors."""
+        g = self._graph
+        if g is None:
+            g = self._graph = {"at": self.at.clone(), "dir": dir.diff.clone(),
+                               "eps": torch.full((), float(eps), dtype=torch.float64, device=self.x0.device),
+                               "atTry": torch.empty_like(self.at), "at_src": self.at, "dir_src": dir.diff}
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side), workspace.scope(self):
+                self._trial_body()          # sizes the private workspaces, initialises lazily created state
+            torch.cuda.current_stream().wait_stream(side)
+            graph = torch.cuda.CUDAGraph()
+            with workspace.scope(self), torch.cuda.graph(graph):
+                g["xt"], g["out"] = self._trial_body()
+            g["graph"] = graph
+        if g["at_src"] is not self.at:
+            g["at"].copy_(self.at)
+            g["at_src"] = self.at
+        if g["dir_src"] is not dir.diff:
+            g["dir"].copy_(dir.diff)
+            g["dir_src"] = dir.diff
+        g["eps"].fill_(float(eps))
+        g["graph"].replay()
+        host = g["out"].cpu().numpy()
+        ereg, data = float(host[0]), float(host[1])
+        objTry = self.obj0 + (ereg + data)
+        if self._auto:
+            objTry = _Value(objTry, self, ereg, g["xt"][-1].clone(), value_bound(self, self._noise, self.obj0))
+        if np.isnan(objTry):
+            logging.info('Warning: nan in updateTry')
+            return 1e500
+        if (objRef is None) or (objTry < objRef):
+            self.atTry = g["atTry"].clone()
+            self.objTry = objTry
+            self.xtTry = g["xt"].clone()
         return objTry
 
     def getGradient(self, coeff=1.0):

@@ -41,7 +41,7 @@ class CurveMatching(DeviceMatching):
     def __init__(self, Template=None, Target=None, fileTempl=None, fileTarg=None, param=None, maxIter=1000,
                  regWeight=1.0, affineWeight=1.0, verb=True, gradLB=0.001, saveRate=10, rotWeight=None,
                  scaleWeight=None, transWeight=None, testGradient=False, saveFile='evolution', affine='none',
-                 outputDir='.', lineSearchPrecision='fp64'):
+                 outputDir='.', lineSearchPrecision='fp64', cudaGraphs=True):
         if Template is None or Target is None:
             raise ValueError('Please provide template and target curves (file readers are not provided)')
         self.fv0 = curves.Curve(curve=Template)
@@ -52,7 +52,8 @@ class CurveMatching(DeviceMatching):
         self.saveRate = saveRate
         self.saveFile = saveFile
         self.outputDir = outputDir
-        self._init_state(maxIter, regWeight, verb, testGradient, affine, False, lineSearchPrecision)
+        self._init_state(maxIter, regWeight, verb, testGradient, affine, False, lineSearchPrecision,
+                         cudaGraphs=cudaGraphs)
 
     @staticmethod
     def shape_copy(c):

@@ -4,7 +4,9 @@ torch provides device memory and streams; all arithmetic happens in the CUDA
 library.  Host numpy arrays are copied to the device as float64 and results are
 copied back as fresh float64 numpy arrays (what the f2py wrapper returned).
 """
+import contextlib
 import ctypes
+import threading
 
 import numpy as np
 import torch
@@ -45,12 +47,30 @@ def stream_handle():
 
 class _WorkspaceCache:
     """One growing uint8 buffer per (device, stream); calls on one stream are
-    ordered, so consecutive calls can reuse it."""
+    ordered, so consecutive calls can reuse it.
+
+    scope(owner) routes the calls made inside it to buffers of their own,
+    one per call position, held by `owner`: a captured CUDA graph keeps
+    pointing at the buffers it was captured with, so they must be neither
+    shared with eager calls nor regrown afterwards."""
 
     def __init__(self):
         self.bufs = {}
+        self._tls = threading.local()
 
     def get(self, nbytes):
+        sc = getattr(self._tls, "scope", None)
+        if sc is not None:
+            owner, pos = sc
+            sc[1] = pos + 1
+            bufs = owner.__dict__.setdefault("_private_workspaces", [])
+            if pos < len(bufs):
+                if bufs[pos].numel() < nbytes:
+                    raise RuntimeError("a scoped workspace cannot grow once captured")
+                return bufs[pos]
+            buf = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+            bufs.append(buf)
+            return buf
         key = (torch.cuda.current_device(), torch.cuda.current_stream().cuda_stream)
         buf = self.bufs.get(key)
         if buf is None or buf.numel() < nbytes:
@@ -60,6 +80,15 @@ class _WorkspaceCache:
             buf = torch.empty(cap, dtype=torch.uint8, device="cuda")
             self.bufs[key] = buf
         return buf
+
+    @contextlib.contextmanager
+    def scope(self, owner):
+        prev = getattr(self._tls, "scope", None)
+        self._tls.scope = [owner, 0]
+        try:
+            yield
+        finally:
+            self._tls.scope = prev
 
     def clear(self):
         self.bufs.clear()

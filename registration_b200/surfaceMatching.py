@@ -9,8 +9,10 @@ errorType selects the (fun_obj0, fun_obj, fun_objGrad) plug-in triple among
 this library's surfaces.current/measure/varifold norms; a user-set triple is
 honoured too (called with Surface objects).  Only affine='none' and
 symmetric=False are provided.  VTK output of the iterates is not written.
-Extra keyword: lineSearchPrecision ('fp64' default) -- the precision of the
-data-term values compared by the line search (see registration_b200._matching).
+Extra keywords: lineSearchPrecision ('fp64' default) -- the precision of the
+data-term values compared by the line search (see registration_b200._matching);
+cudaGraphs (True) -- replay each line-search trial (shot + data-term value)
+from a captured CUDA graph instead of launching its kernels one by one.
 """
 import logging
 
@@ -48,7 +50,7 @@ class SurfaceMatching(DeviceMatching):
     def __init__(self, Template=None, Target=None, fileTempl=None, fileTarg=None, param=None, maxIter=1000,
                  regWeight=1.0, affineWeight=1.0, verb=True, subsampleTargetSize=-1, rotWeight=None,
                  scaleWeight=None, transWeight=None, symmetric=False, testGradient=True, saveFile='evolution',
-                 affine='none', outputDir='.', lineSearchPrecision='fp64'):
+                 affine='none', outputDir='.', lineSearchPrecision='fp64', cudaGraphs=True):
         if Template is None:
             if fileTempl is None:
                 raise ValueError('Please provide a template surface')
@@ -70,7 +72,8 @@ class SurfaceMatching(DeviceMatching):
             self.fv1.flipFaces()
         self.fvInit = surfaces.Surface(surf=self.fv0)
         self.fvDef = surfaces.Surface(surf=self.fvInit)
-        self._init_state(maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision)
+        self._init_state(maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision,
+                         cudaGraphs=cudaGraphs)
         self.coeffAff1 = 1.
         self.coeffAff2 = 100.
         self.coeffAff = self.coeffAff1

@@ -115,3 +115,37 @@ def test_matching_from_mesh_files(golden, tmp_path):
     b.optimizeMatching()
     assert float(a.obj) == float(b.obj)
     assert bool((a.at == b.at).all())
+
+
+@pytest.mark.parametrize("case", ["surface-auto", "surface-fp64", "curve-fp32c"])
+def test_graphed_trials_equal_eager_trials(golden, case):
+    """cudaGraphs=True replays the same kernels on the same inputs: the traces
+    and the momenta are bit-identical to the eager path."""
+    from registration_b200 import curveMatching as CM
+    from registration_b200 import curves as cv
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+    runs = []
+    for graphs in (False, True):
+        if case.startswith("surface"):
+            prec = "fp64" if case.endswith("fp64") else "fp32c"
+            f, v0, v1 = golden["sm_faces"], golden["sm_v0"], golden["sm_v1"]
+            param = SM.SurfaceMatchingParam(timeStep=0.2, KparDiff=kf.Kernel(name="gauss", sigma=0.4, precision=prec),
+                                            KparDist=kf.Kernel(name="gauss", sigma=0.3, precision=prec),
+                                            sigmaError=0.5, errorType="varifold")
+            m = SM.SurfaceMatching(Template=sf.Surface(FV=[f, v0]), Target=sf.Surface(FV=[f, v1]), param=param,
+                                   maxIter=6, testGradient=True, lineSearchPrecision="auto" if prec == "fp32c" else "fp64",
+                                   cudaGraphs=graphs)
+        else:
+            param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5),
+                                          KparDist=kf.Kernel(name="gauss", sigma=0.5), sigmaError=1.0,
+                                          errorType="current")
+            m = CM.CurveMatching(Template=cv.Curve(pointSet=golden["cm_v0"]), Target=cv.Curve(pointSet=golden["cm_v1"]),
+                                 param=param, maxIter=8, saveRate=0, lineSearchPrecision="fp32c", cudaGraphs=graphs)
+        trace = _trace(m)
+        m.optimizeMatching()
+        runs.append((trace, m.at.clone(), float(m.obj), dict(m.calls)))
+    (t0, a0, o0, c0), (t1, a1, o1, c1) = runs
+    assert t0 == t1 and o0 == o1 and c0 == c1
+    assert bool((a0 == a1).all())
