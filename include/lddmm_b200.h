@@ -272,7 +272,11 @@ LDDMM_API int lddmm_applykdiff11and12_f64(const double* x, int64_t n, int d, con
  * each segment computes exactly what the single-problem entry point above
  * computes for its own rows, with its own kernel width, and its results do not
  * depend on the other segments of the launch (per-segment chunking and FP64
- * reduction trees).  Offsets / sigma / regweight arrays are HOST arrays.
+ * reduction trees).  Offsets / sigma / regweight arrays are HOST arrays; the
+ * segment tables built from them are copied to the device by each call, so a
+ * call on a stream that is capturing a CUDA graph is refused (LDDMM_ERR_ARG)
+ * before anything is enqueued.  The single-problem entry points above enqueue
+ * only kernels, device-to-device copies and memsets and can be captured.
  *
  * Shooting / adjoint of nreq requests, request s owning points
  * [v_off[s], v_off[s+1]) (v_off has nreq+1 entries, v_off[0] = 0):

@@ -30,6 +30,7 @@ import numpy as np
 import torch
 
 from . import _dataterm as _dt
+from . import _ragged as _rg
 from . import pointEvolution as evol
 from ._precision import _Value, value_bound
 from .device import require_cuda, to_dev, workspace
@@ -203,14 +204,21 @@ class DeviceMatching:
             g = self._graph = {"at": self.at.clone(), "dir": dir.diff.clone(),
                                "eps": torch.full((), float(eps), dtype=torch.float64, device=self.x0.device),
                                "atTry": torch.empty_like(self.at), "at_src": self.at, "dir_src": dir.diff}
+            # capture on a side stream with the low-level calls (the torch.cuda.graph
+            # context manager also collects garbage and empties the allocator cache)
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(side), workspace.scope(self):
-                self._trial_body()          # sizes the private workspaces, initialises lazily created state
-            torch.cuda.current_stream().wait_stream(side)
             graph = torch.cuda.CUDAGraph()
-            with workspace.scope(self), torch.cuda.graph(graph):
-                g["xt"], g["out"] = self._trial_body()
+            with torch.cuda.stream(side):
+                with workspace.scope(self):
+                    self._trial_body()      # sizes the private workspaces, initialises lazily created state
+                with workspace.scope(self):
+                    graph.capture_begin()
+                    try:
+                        g["xt"], g["out"] = self._trial_body()
+                    finally:
+                        graph.capture_end()
+            torch.cuda.current_stream().wait_stream(side)
             g["graph"] = graph
         if g["at_src"] is not self.at:
             g["at"].copy_(self.at)
@@ -265,8 +273,15 @@ class DeviceMatching:
     def dotProduct(self, g1, g2):
         """sum_t <g2_t, K(x_t) g1_t> (surfaceMatching.py:353-377), FP64 on the device."""
         self.calls["dotProduct"] += 1
-        acc = torch.zeros(len(g2), dtype=torch.float64, device=self.x0.device)
         K = self.param.KparDiff
+        if K.precision == 'fp32c':
+            # the T applyK sums as one ragged launch (one segment per time step)
+            T, N, d = self.Tsize, self.npt, self.dim
+            U = _rg.applyk_segments(self.xt[:T].reshape(-1, d), to_dev(g1.diff).reshape(-1, d),
+                                    [t * N for t in range(T)], [N] * T, [K.sigma] * T, _rg.kernel_order(K))
+            G2 = torch.stack([to_dev(gr.diff).reshape(-1) for gr in g2])
+            return (G2 @ U.reshape(-1)).cpu().numpy()
+        acc = torch.zeros(len(g2), dtype=torch.float64, device=self.x0.device)
         for t in range(self.Tsize):
             u = K.applyK(self.xt[t], g1.diff[t])
             for ll, gr in enumerate(g2):

@@ -54,7 +54,10 @@ def cg(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=10.):
             epsfoo = 1e-7
             objfoo = opt.updateTry(dirfoo, epsfoo, obj - 1e10)
             [grdfoo] = dot(grd, [dirfoo])
-            logging.info('Test Gradient: %.4f %.4f' % ((objfoo - obj) / epsfoo, -grdfoo * gradCoeff))
+            # only logged: the difference is formed (and, for values with an
+            # error bound, refined) only when the log line is emitted
+            if logging.getLogger().isEnabledFor(logging.INFO):
+                logging.info('Test Gradient: %.4f %.4f' % ((objfoo - obj) / epsfoo, -grdfoo * gradCoeff))
         if it == 0 or it == cgBurnIn:
             [grdOld2] = dot(grd, [grd])
             grd2 = grdOld2

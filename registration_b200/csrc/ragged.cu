@@ -876,11 +876,19 @@ int rag_run(Run run, void* wsp, size_t wsb, cudaStream_t st, const char* who) {
         set_error("%s: workspace too small: need %zu bytes, got %zu", who, meas.off, wsb);
         return LDDMM_ERR_WORKSPACE;
     }
+    // The segment tables are built on the host and copied to the device with
+    // each call; a CUDA graph would keep the host address of that copy, so a
+    // capturing stream is refused before anything is enqueued.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    LDDMM_TRY(cuda_check(cudaStreamIsCapturing(st, &cap), who));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("%s: ragged entry points cannot be captured into a CUDA graph (host-built segment tables)", who);
+        return LDDMM_ERR_ARG;
+    }
     LDDMM_TRY(check_device_ptr(wsp, "workspace"));
     Workspace ws;
     ws.base = static_cast<char*>(wsp);
     ws.cap = wsb;
-    (void)st;
     return run(ws);
 }
 

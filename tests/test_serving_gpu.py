@@ -322,3 +322,26 @@ def test_serving_matches_single_problem_driver():
         # small difference of norms -- agrees to the FP32c bar, 1e-5 relative
         assert res["iters"] == sm.iter
         assert abs(res["obj"] - sm.obj) <= 1e-5 * abs(sm.obj), (res["obj"], sm.obj)
+
+
+def test_ragged_call_refused_while_capturing():
+    """Ragged entry points copy host-built segment tables to the device on each
+    call; on a stream that is capturing a CUDA graph they return an error
+    before enqueueing anything (a captured copy would keep a stale host address)."""
+    import torch
+    from registration_b200 import _ragged as rg
+    x = torch.rand(64, 3, dtype=torch.float64, device="cuda")
+    a = torch.rand(64, 3, dtype=torch.float64, device="cuda")
+    rg.applyk_segments(x, a, [0, 32], [32, 32], [0.3, 0.3], 10)   # eager: fine
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        try:
+            with pytest.raises(ValueError, match="captured"):
+                rg.applyk_segments(x, a, [0, 32], [32, 32], [0.3, 0.3], 10)
+        finally:
+            g.capture_end()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
