@@ -190,3 +190,22 @@ def test_second_derivative_loops_random_sizes(oracle_lib, kf, precision, name, o
     assert _err(K.applyDDiffK12(x, a1, a2, p), oracle_lib.applykdiff12(x, a1, a2, p, 0.1, o)) < TOL[precision]
     assert _err(K.applyDDiffK11and12(x, a1, a2, p),
                 oracle_lib.applykdiff11and12(x, a1, a2, p, 0.1, o)) < TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+def test_empty_inputs(kf, precision):
+    """No targets -> an empty result; no sources -> zeros (the f2py loops'
+    results for num_nodes = 0 / num_nodes_y = 0)."""
+    rng = np.random.default_rng(2)
+    K = kf.Kernel(name="gauss", sigma=0.3, precision=precision)
+    x = rng.uniform(0, 1, (0, 3))
+    y = rng.uniform(0, 1, (17, 3))
+    a = rng.standard_normal((17, 3))
+    f = K.applyK(y, a, firstVar=x)
+    assert f.shape == (0, 3)
+    f = K.applyDiffKT(y, [np.zeros((0, 3))], [a], firstVar=x)
+    assert f.shape == (0, 3)
+    f = K.applyK(np.zeros((0, 3)), np.zeros((0, 2)), firstVar=y)
+    assert f.shape == (17, 2) and not f.any()
+    f = K.applyDiffKT(np.zeros((0, 3)), [rng.standard_normal((17, 3))], [np.zeros((0, 3))], firstVar=y)
+    assert f.shape == (17, 3) and not f.any()
