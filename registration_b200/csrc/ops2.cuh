@@ -78,13 +78,16 @@ LDDMM_D f2 kdiff2(const unsigned long long* pqd, f2 r2) {
     }
 }
 
-template <int KIND, int DEG, int D, int DIMB>
+// SMALL: tile shape for a few thousand targets or fewer (64 targets per
+// 32-thread block, 32-source tiles), so that the (target block, source chunk)
+// items spread over the SMs instead of filling one or two 512-target blocks.
+template <int KIND, int DEG, int D, int DIMB, bool SMALL = false>
 struct OpApplyK2 {
     using Real = float;
     static constexpr bool F32 = true;
     static constexpr bool DUP = true;
     static constexpr int TPS = 2;
-    static constexpr int BLOCK = 128, R = 4, TILE = 128, FOLD = 32;
+    static constexpr int BLOCK = SMALL ? 32 : 128, R = SMALL ? 2 : 4, TILE = SMALL ? 32 : 128, FOLD = 32;
     static constexpr int PP = 1;            // target planes: pos
     static constexpr int NV = D + DIMB;     // source values
     static constexpr int NS = (NV + 1) / 2; // source words (duplicated values)
@@ -114,13 +117,13 @@ struct OpApplyK2 {
     }
 };
 
-template <int KIND, int DEG, int D, int W>
+template <int KIND, int DEG, int D, int W, bool SMALL = false>
 struct OpDiffKT2 {
     using Real = float;
     static constexpr bool F32 = true;
     static constexpr bool DUP = true;
     static constexpr int TPS = 2;
-    static constexpr int BLOCK = 128, R = 4, TILE = 128, FOLD = 32;
+    static constexpr int BLOCK = SMALL ? 32 : 128, R = SMALL ? 2 : 4, TILE = SMALL ? 32 : 128, FOLD = 32;
     static constexpr int PP = 1;
     static constexpr int NV = D + W;
     static constexpr int NS = (NV + 1) / 2;

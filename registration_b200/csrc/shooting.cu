@@ -187,10 +187,10 @@ struct ShootArgs {
     double* energy;
 };
 
-template <class Real, int KIND, int DEG, int D>
+template <class Real, int KIND, int DEG, int D, bool SMALL = false>
 int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr bool DUP = sizeof(Real) == 4;  // FP32: packed-pair operator with duplicated sources
-    using Op = std::conditional_t<DUP, OpApplyK2<KIND, DEG, D, D>, OpApplyK<Real, KIND, DEG, D, D>>;
+    using Op = std::conditional_t<DUP, OpApplyK2<KIND, DEG, D, D, SMALL>, OpApplyK<Real, KIND, DEG, D, D>>;
     const SinglePlan pl = plan_single<Op>(a.n, a.n);
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
@@ -228,7 +228,11 @@ template <class Real>
 int shoot_run(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     return dispatch_kind_p(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
-            return shoot_impl<Real, decltype(kind)::value, decltype(deg)::value, decltype(D)::value>(a, ws, st);
+            constexpr int K_ = decltype(kind)::value, P_ = decltype(deg)::value, D_ = decltype(D)::value;
+            if constexpr (sizeof(Real) == 4) {
+                if (a.n <= kSmallTargets) return shoot_impl<Real, K_, P_, D_, true>(a, ws, st);
+            }
+            return shoot_impl<Real, K_, P_, D_>(a, ws, st);
         });
     });
 }
@@ -318,11 +322,11 @@ struct CovArgs {
     double* dat;
 };
 
-template <class Real, int KIND, int DEG, int D>
+template <class Real, int KIND, int DEG, int D, bool SMALL = false>
 int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr int W = 2 * D;
     constexpr bool DUP = sizeof(Real) == 4;  // FP32: packed-pair operator with duplicated sources
-    using Op = std::conditional_t<DUP, OpDiffKT2<KIND, DEG, D, W>, OpDiffKT<Real, KIND, DEG, D, W>>;
+    using Op = std::conditional_t<DUP, OpDiffKT2<KIND, DEG, D, W, SMALL>, OpDiffKT<Real, KIND, DEG, D, W>>;
     constexpr int NT = DUP ? 1 + (W + 3) / 4 : Op::NS;  // target planes (standard layout)
     const SinglePlan pl = plan_single<Op>(a.n, a.n);
     float4* tgt = ws.take<float4>((size_t)NT * pl.n_tpad);
@@ -362,7 +366,11 @@ template <class Real>
 int cov_run(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     return dispatch_kind_q(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
-            return cov_impl<Real, decltype(kind)::value, decltype(deg)::value, decltype(D)::value>(a, ws, st);
+            constexpr int K_ = decltype(kind)::value, Q_ = decltype(deg)::value, D_ = decltype(D)::value;
+            if constexpr (sizeof(Real) == 4) {
+                if (a.n <= kSmallTargets) return cov_impl<Real, K_, Q_, D_, true>(a, ws, st);
+            }
+            return cov_impl<Real, K_, Q_, D_>(a, ws, st);
         });
     });
 }

@@ -19,6 +19,11 @@ int sweep_slots() {
     return 8 * device_info().sms;
 }
 
+// Problems with at most this many targets use the SMALL tile shape of the
+// packed operators that have one (more, smaller items: the large shape would
+// leave most SMs idle).
+constexpr long long kSmallTargets = 4096;
+
 struct SinglePlan {
     long long n_tpad, m_pad;
     int n_tb, n_src_tiles, split;

@@ -50,7 +50,7 @@ def test_evolution_golden(golden, oracle_lib, mods, precision, kname):
 
 @pytest.mark.parametrize("precision", ["fp32c", "fp64"])
 @pytest.mark.parametrize("kname,order,sigma", [("gauss", 10, 0.2), ("laplacian", 3, 0.25)])
-@pytest.mark.parametrize("n,d,T", [(3000, 3, 10), (2500, 2, 7), (1, 3, 3), (777, 1, 4)])
+@pytest.mark.parametrize("n,d,T", [(3000, 3, 10), (2500, 2, 7), (1, 3, 3), (777, 1, 4), (6000, 3, 3)])
 def test_shoot_covector_against_oracle(oracle_lib, mods, precision, kname, order, sigma, n, d, T):
     from oracle import lddmm_ref as ref
     kf, ev = mods
