@@ -84,45 +84,6 @@ LDDMM_D void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Bulk copies on the copy engine (TMA), completing on a shared-memory
-// mbarrier: one thread arms the barrier with the byte count and issues the
-// copies; every thread waits for the barrier's phase.  No multicast.
-LDDMM_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-LDDMM_D void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-LDDMM_D void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-LDDMM_D void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
-LDDMM_D void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-LDDMM_D bool mbar_test(unsigned long long* bar, unsigned parity) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-// Polls of a bounded wait (about a second at most): a copy that has not
-// completed by then never will, and the caller gives up instead of hanging.
-constexpr int kWaitPolls = 1 << 24;
-LDDMM_D bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (int i = 0; i < kWaitPolls; ++i) {
-        if (mbar_test(bar, parity)) return true;
-        if (i >= 32) __nanosleep(32);
-    }
-    return false;
-}
-
 struct double4a {  // 32-byte record of four doubles
     double x, y, z, w;
 };

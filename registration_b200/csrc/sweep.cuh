@@ -3,12 +3,8 @@
 // Each block owns BLOCK*R targets (R per thread, kept in registers) and one
 // chunk of the source range.  Source records (NS 16-byte words each, packed
 // structure-of-arrays in global memory, see Op::Src) are streamed through
-// shared memory in tiles of TILE records, double-buffered: for each tile one
-// thread issues NS bulk copies (one contiguous plane each, cp.async.bulk on the
-// copy engine) that complete on the stage's mbarrier, while the block computes
-// on the other stage; every warp reads the same record at the same time
-// (shared-memory broadcast).  The waits are bounded: if a copy has not
-// completed after about a second the block writes NaN sums and leaves.
+// shared memory in tiles of TILE records with a two-stage cp.async pipeline;
+// every warp reads the same record at the same time (shared-memory broadcast).
 // Per-target accumulators: FP32 partials over FOLD sources, folded into a
 // TwoSum-compensated (sum, err) pair (FP32 ops), or plain FP64 sums.
 // The block writes its per-target sums as doubles into the partial buffer
@@ -36,16 +32,7 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
     constexpr int WORDS_PER_REC = NS;                  // 16-byte words per source record
     constexpr int WORDS_PER_TILE = WORDS_PER_REC * TILE;
     static_assert(WORDS_PER_TILE % BLOCK == 0, "tile must split evenly over the block");
-    __shared__ __align__(128) float4 smem[2][WORDS_PER_TILE];
-    __shared__ __align__(8) unsigned long long full[2];   // one mbarrier per stage
-    __shared__ int timed_out;
-    if (threadIdx.x == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-        mbar_init_fence();
-        timed_out = 0;
-    }
-    __syncthreads();
+    __shared__ __align__(16) float4 smem[2][WORDS_PER_TILE];
 
     const int item = blockIdx.x;
     const SegDesc sg = find_segment(grid, item);
@@ -80,38 +67,28 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
     for (int q = 0; q < SLOTS; ++q) acc[q].zero();
 
     // global source words: Op lays a record out as NS planes of float4 words,
-    // plane p of record j at P.src4[p * P.src_stride + j]; a tile of plane p is
-    // TILE contiguous words, copied to smem[stage][p * TILE ...]
+    // plane p of record j at P.src4[p * P.src_stride + j]
     auto load_tile = [&](int tile, int stage) {
-        if (threadIdx.x == 0) {
-            const long long rec0 = sg.src + (long long)tile * TILE;
-            mbar_expect_tx(&full[stage], (unsigned)(WORDS_PER_TILE * 16));
+        const long long rec0 = sg.src + (long long)tile * TILE;
 #pragma unroll
-            for (int p = 0; p < NS; ++p)
-                bulk_g2s(&smem[stage][p * TILE], P.src4 + (long long)p * P.src_stride + rec0, TILE * 16,
-                         &full[stage]);
+        for (int w = threadIdx.x; w < WORDS_PER_TILE; w += BLOCK) {
+            const int plane = w / TILE;
+            const int j = w - plane * TILE;
+            cp_async16(&smem[stage][w], P.src4 + (long long)plane * P.src_stride + rec0 + j);
         }
+        cp_async_commit();
     };
 
-    bool ok = true;
     if (tile_lo < tile_hi) load_tile(tile_lo, 0);
     for (int tile = tile_lo; tile < tile_hi; ++tile) {
-        const int i = tile - tile_lo;
-        const int stage = i & 1;
-        // stage^1 was last read in the previous iteration, which ended on a barrier
-        if (tile + 1 < tile_hi) load_tile(tile + 1, stage ^ 1);
-        if (!mbar_wait_bounded(&full[stage], (unsigned)((i >> 1) & 1))) timed_out = 1;
-        __syncthreads();
-        if (timed_out) {
-            // let the copies in flight finish (bounded) before the block's shared memory is released
-            if (threadIdx.x == 0) {
-                mbar_wait_bounded(&full[stage], (unsigned)((i >> 1) & 1));
-                if (tile + 1 < tile_hi) mbar_wait_bounded(&full[stage ^ 1], (unsigned)(((i + 1) >> 1) & 1));
-            }
-            __syncthreads();
-            ok = false;
-            break;
+        const int stage = (tile - tile_lo) & 1;
+        if (tile + 1 < tile_hi) {
+            load_tile(tile + 1, stage ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
+        __syncthreads();
         const float4* S = smem[stage];
         const float wt = (SYM && tile >= diag_hi && tile < sg.sym_tiles) ? 2.f : 1.f;
         (void)wt;
@@ -144,8 +121,7 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
                 double* dst = part + (sg.part + (long long)chunk * sg.n_tgt + t) * NOUT;
 #pragma unroll
                 for (int c = 0; c < NOUT; ++c) {
-                    if (!ok) dst[c] = __longlong_as_double(0x7ff8000000000000LL);   // NaN: the sums are incomplete
-                    else if constexpr (TPS == 1) dst[c] = acc[q].value(c);
+                    if constexpr (TPS == 1) dst[c] = acc[q].value(c);
                     else dst[c] = acc[q].value(c, lane);
                 }
             }
