@@ -53,6 +53,11 @@ from .device import require_cuda
 NORMS = _rg.NORMS
 
 
+def _volume(v, f):
+    """Signed volume sum_f det(v0, v1, v2) / 6 (surfaces.py:711-717)."""
+    return float((np.linalg.det(v[f]) / 6).sum())
+
+
 class MatchRequest:
     """One matching problem.
 
@@ -73,6 +78,13 @@ class MatchRequest:
             raise ValueError("template and target must have the same cell size and dimension")
         if param.errorType == "varifold" and self.f0.shape[1] != 3:
             raise ValueError("the varifold norm is defined for triangulated surfaces")
+        if self.f0.shape[1] == 3 and self.v0.shape[1] == 3:
+            # SurfaceMatching orients the target like the template (surfaceMatching.py:126-129)
+            if _volume(self.v0, self.f0) * _volume(self.v1, self.f1) < 0:
+                self.f1 = np.ascontiguousarray(self.f1[:, [0, 2, 1]])
+        # cg's first step: SurfaceMatching passes epsInit = 0.1 (surfaceMatching.py:484),
+        # CurveMatching keeps cg's default 10 (curveMatching.py:352)
+        self.eps_init = 0.1 if self.f0.shape[1] == 3 else 10.0
         self.param = param
         self.T = int(round(1.0 / param.timeStep))
         self.max_iter = int(maxIter)
@@ -303,11 +315,13 @@ class Scheduler:
                     lane.active.discard(slot)
                     lane.active.add(prob)
                     self.cv.notify_all()
-                # SurfaceMatching.optimizeMatching (surfaceMatching.py:474-484)
+                # SurfaceMatching / CurveMatching.optimizeMatching (surfaceMatching.py:474-484,
+                # curveMatching.py:342-352: gradEps = max(1e-3, |g| / 1e4))
                 grd = prob.getGradient(prob.gradCoeff)
                 [g2] = prob.dotProduct(grd, [grd])
                 prob.gradEps = max(0.001, np.sqrt(g2) / 10000)
-                cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False, epsInit=0.1)
+                cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False,
+                      epsInit=getattr(req, "eps_init", 0.1))
                 obj = prob.obj.refine() if isinstance(prob.obj, _Value) else float(prob.obj)
                 req.result = {"at": prob.at, "xt": prob.xt, "obj": obj, "iters": prob.iters,
                               "converged": prob.converged, "calls": dict(prob.calls)}

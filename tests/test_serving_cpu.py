@@ -261,3 +261,26 @@ def test_match_request_validation(bad):
         errorType = "hausdorff"
     with pytest.raises(ValueError):
         serving.MatchRequest(None, None, P())
+
+
+def test_match_request_orients_target_and_picks_the_protocol_step():
+    """A surface target with the opposite orientation gets its faces flipped, as
+    SurfaceMatching does (surfaceMatching.py:126-129); curves keep cg's default
+    first step (epsInit 10, curveMatching.py:352), surfaces use 0.1."""
+    from registration_b200 import curves as cv
+    from registration_b200 import geometry as geo
+    from registration_b200 import surfaces as sf
+
+    class P:
+        timeStep = 0.2
+        errorType = "current"
+    v, f = geo.icosphere(1)
+    inward = f[:, [0, 2, 1]]
+    r = serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[inward, 1.1 * v]), P())
+    np.testing.assert_array_equal(r.f1, f)
+    assert r.eps_init == 0.1
+    same = serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[f, 1.1 * v]), P())
+    np.testing.assert_array_equal(same.f1, f)
+    c, _ = geo.ellipse_curve(32)
+    rc = serving.MatchRequest(cv.Curve(pointSet=c), cv.Curve(pointSet=1.1 * c), P())
+    assert rc.f0.shape[1] == 2 and rc.eps_init == 10.0

@@ -345,3 +345,42 @@ def test_ragged_call_refused_while_capturing():
             g.capture_end()
     torch.cuda.current_stream().wait_stream(s)
     torch.cuda.synchronize()
+
+
+def _curve_requests(idx, iters=8):
+    from registration_b200 import curves as cv
+    from registration_b200 import geometry as geo
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import serving
+    from registration_b200.curveMatching import CurveMatchingParam
+    out = []
+    for i in idx:
+        rng = np.random.default_rng(40 + i)
+        v, _ = geo.ellipse_curve(64 + 32 * i, 1.0, 0.6)
+        vt, _ = geo.bumped_curve(v, 3, 0.3, 0.1, rng)
+        param = CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5),
+                                   KparDist=kf.Kernel(name="gauss", sigma=0.5), sigmaError=0.2,
+                                   errorType="current")
+        out.append(serving.MatchRequest(cv.Curve(pointSet=v), cv.Curve(pointSet=vt), param, maxIter=iters, rid=i))
+    return out
+
+
+def test_served_curves_alone_equal_mix_and_match_curve_matching():
+    """Curve requests (edges, d = 2) follow CurveMatching's protocol (cg's
+    first step 10): alone == in the mix bit for bit, and the same decisions as
+    the single-problem CurveMatching with FP64 line-search values."""
+    from registration_b200 import curves as cv
+    from registration_b200 import serving
+    from registration_b200.curveMatching import CurveMatching
+    mix = _curve_requests(range(3))
+    serving.serve(mix, line_search_precision="fp64")
+    for r in mix:
+        alone = _curve_requests([r.rid])
+        serving.serve(alone, line_search_precision="fp64")
+        a, b = _result(alone[0]), _result(r)
+        assert a["obj"] == b["obj"] and torch.equal(a["at"], b["at"])
+        cm = CurveMatching(Template=cv.Curve(pointSet=r.v0), Target=cv.Curve(pointSet=r.v1), param=r.param,
+                           maxIter=8, saveRate=0, lineSearchPrecision="fp64")
+        cm.optimizeMatching()
+        assert b["iters"] == cm.iter
+        assert abs(b["obj"] - cm.obj) <= 1e-5 * abs(cm.obj), (b["obj"], cm.obj)
