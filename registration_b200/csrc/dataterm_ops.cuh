@@ -48,13 +48,13 @@ struct DataLayout {
                                                       : D + 1;
 };
 
-template <class Real_, int KIND, int PDEG, int QDEG, int D, int MODE>
+template <class Real_, int KIND, int PDEG, int QDEG, int D, int MODE, bool SMALL = false>
 struct OpData {
     using Real = Real_;
     using L = DataLayout<MODE, D>;
     static constexpr bool F32 = sizeof(Real) == 4;
     static constexpr int TPS = 1;
-    static constexpr int BLOCK = 128, R = 2, TILE = 128, FOLD = F32 ? 32 : TILE;
+    static constexpr int BLOCK = SMALL ? 32 : 128, R = 2, TILE = SMALL ? 32 : 128, FOLD = F32 ? 32 : TILE;
     static constexpr int PP = PointPlanes<Real>::N;
     static constexpr int PW = Traits<Real>::PER_WORD;
     static constexpr int TVW = (L::TV + PW - 1) / PW;

@@ -78,7 +78,9 @@ struct DtOp : Base {
     static constexpr int SSLOTS = SSLOTS_;
 };
 
-template <class Real, int KIND, int PDEG, int QDEG, int D>
+// SMALL: the small tile shape for the unpacked operators (few target cells);
+// the packed FP32 surface operators keep their shape.
+template <class Real, int KIND, int PDEG, int QDEG, int D, bool SMALL = false>
 int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr int PW = Traits<Real>::PER_WORD;
     constexpr int PP = PointPlanes<Real>::N;
@@ -100,16 +102,16 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
         if (a.norm == NVARIFOLD) {
             // FP32: packed-pair operator (two targets per slot, duplicated sources)
             using Op = std::conditional_t<(sizeof(Real) == 4 && D == 3), DtOp<OpVariValue2<KIND, PDEG>, 3, 4, 2>,
-                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE>, 3, 4,
+                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_VALUE, SMALL>, 3, 4,
                                                PP + (3 + PW - 1) / PW>>;
             rc = dt_sweep<Op, Real, true>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else if (a.norm == NCURRENT) {
-            using Op = DtOp<OpApplyK<Real, KIND, PDEG, D, D>, 0, D, PP>;
+            using Op = DtOp<OpApplyK<Real, KIND, PDEG, D, D, SMALL>, 0, D, PP>;
             rc = dt_sweep<Op, Real, true>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else {
-            using Op = DtOp<OpApplyK<Real, KIND, PDEG, D, 1>, 0, 1, PP>;
+            using Op = DtOp<OpApplyK<Real, KIND, PDEG, D, 1, SMALL>, 0, 1, PP>;
             rc = dt_sweep<Op, Real, true>(a, ws, st, 0, -2.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         }
@@ -129,18 +131,18 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
         constexpr bool PACK = sizeof(Real) == 4 && D == 3;   // FP32 surfaces: packed-pair operators
         if (a.norm == NVARIFOLD) {
             using Op = std::conditional_t<PACK, DtOp<OpVariGrad2<KIND, PDEG, QDEG>, 3, 4, 2>,
-                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_GRAD>, 3, 4,
+                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_VARI_GRAD, SMALL>, 3, 4,
                                                PP + (3 + PW - 1) / PW>>;
             rc = dt_sweep<Op, Real>(a, ws, st, 1, -1.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else if (a.norm == NCURRENT) {
             using Op = std::conditional_t<PACK, DtOp<OpCurGrad2<KIND, PDEG, QDEG>, D, D, 2>,
-                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_CUR_GRAD>, D, D,
+                                          DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_CUR_GRAD, SMALL>, D, D,
                                                PP + (D + PW - 1) / PW>>;
             rc = dt_sweep<Op, Real>(a, ws, st, 1, -1.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         } else {
-            using Op = DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_MEAS_GRAD>, 0, 1, PP>;
+            using Op = DtOp<OpData<Real, KIND, PDEG, QDEG, D, M_MEAS_GRAD, SMALL>, 0, 1, PP>;
             rc = dt_sweep<Op, Real>(a, ws, st, 1, -1.0, c1, s1, part, pl, ks, center);
             nout = Op::NOUT;
         }
@@ -163,8 +165,10 @@ template <class Real>
 int dt_run(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     auto go = [&](auto kind, auto pdeg, auto qdeg) {
         return dispatch_d(a.d, [&](auto D) {
-            return dt_impl<Real, decltype(kind)::value, decltype(pdeg)::value, decltype(qdeg)::value,
-                           decltype(D)::value>(a, ws, st);
+            constexpr int K_ = decltype(kind)::value, P_ = decltype(pdeg)::value, Q_ = decltype(qdeg)::value,
+                          D_ = decltype(D)::value;
+            if (a.nc <= kSmallTargets) return dt_impl<Real, K_, P_, Q_, D_, true>(a, ws, st);
+            return dt_impl<Real, K_, P_, Q_, D_>(a, ws, st);
         });
     };
     switch (a.order) {

@@ -109,14 +109,16 @@ struct PointPlanes {
 // ---------------------------------------------------------------------------
 // f_k = sum_l K(x_k, y_l) beta_l
 // ---------------------------------------------------------------------------
-template <class Real_, int KIND, int DEG, int D, int DIMB>
+// SMALL: 32-thread blocks and 32-record tiles for a few thousand targets or
+// fewer (see OpApplyK2 in ops2.cuh)
+template <class Real_, int KIND, int DEG, int D, int DIMB, bool SMALL = false>
 struct OpApplyK {
     using Real = Real_;
     static constexpr bool F32 = sizeof(Real) == 4;
     static constexpr int TPS = 1;
-    static constexpr int BLOCK = 128;
-    static constexpr int R = F32 ? 4 : 2;
-    static constexpr int TILE = 128;
+    static constexpr int BLOCK = SMALL ? 32 : 128;
+    static constexpr int R = (F32 && !SMALL) ? 4 : 2;
+    static constexpr int TILE = SMALL ? 32 : 128;
     static constexpr int FOLD = F32 ? 32 : TILE;
     static constexpr int PP = PointPlanes<Real>::N;
     static constexpr int WP = (DIMB + Traits<Real>::PER_WORD - 1) / Traits<Real>::PER_WORD;
@@ -154,14 +156,14 @@ struct OpApplyK {
 // ---------------------------------------------------------------------------
 // f_k = sum_l K'(x_k,y_l) 2 (x_k - y_l) <u_k, v_l>     (up to the combine scale)
 // ---------------------------------------------------------------------------
-template <class Real_, int KIND, int DEG, int D, int W>
+template <class Real_, int KIND, int DEG, int D, int W, bool SMALL = false>
 struct OpDiffKT {
     using Real = Real_;
     static constexpr bool F32 = sizeof(Real) == 4;
     static constexpr int TPS = 1;
-    static constexpr int BLOCK = 128;
+    static constexpr int BLOCK = SMALL ? 32 : 128;
     static constexpr int R = 2;
-    static constexpr int TILE = 128;
+    static constexpr int TILE = SMALL ? 32 : 128;
     static constexpr int FOLD = F32 ? 32 : TILE;
     static constexpr int PP = PointPlanes<Real>::N;
     static constexpr int WP = (W + Traits<Real>::PER_WORD - 1) / Traits<Real>::PER_WORD;

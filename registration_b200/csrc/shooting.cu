@@ -190,7 +190,7 @@ struct ShootArgs {
 template <class Real, int KIND, int DEG, int D, bool SMALL = false>
 int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr bool DUP = sizeof(Real) == 4;  // FP32: packed-pair operator with duplicated sources
-    using Op = std::conditional_t<DUP, OpApplyK2<KIND, DEG, D, D, SMALL>, OpApplyK<Real, KIND, DEG, D, D>>;
+    using Op = std::conditional_t<DUP, OpApplyK2<KIND, DEG, D, D, SMALL>, OpApplyK<Real, KIND, DEG, D, D, SMALL>>;
     const SinglePlan pl = plan_single<Op>(a.n, a.n);
     float4* tgt = ws.take<float4>((size_t)Op::PP * pl.n_tpad);
     float4* src = ws.take<float4>((size_t)Op::NS * pl.m_pad);
@@ -229,9 +229,7 @@ int shoot_run(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     return dispatch_kind_p(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(deg)::value, D_ = decltype(D)::value;
-            if constexpr (sizeof(Real) == 4) {
-                if (a.n <= kSmallTargets) return shoot_impl<Real, K_, P_, D_, true>(a, ws, st);
-            }
+            if (a.n <= kSmallTargets) return shoot_impl<Real, K_, P_, D_, true>(a, ws, st);
             return shoot_impl<Real, K_, P_, D_>(a, ws, st);
         });
     });
@@ -326,7 +324,7 @@ template <class Real, int KIND, int DEG, int D, bool SMALL = false>
 int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     constexpr int W = 2 * D;
     constexpr bool DUP = sizeof(Real) == 4;  // FP32: packed-pair operator with duplicated sources
-    using Op = std::conditional_t<DUP, OpDiffKT2<KIND, DEG, D, W, SMALL>, OpDiffKT<Real, KIND, DEG, D, W>>;
+    using Op = std::conditional_t<DUP, OpDiffKT2<KIND, DEG, D, W, SMALL>, OpDiffKT<Real, KIND, DEG, D, W, SMALL>>;
     constexpr int NT = DUP ? 1 + (W + 3) / 4 : Op::NS;  // target planes (standard layout)
     const SinglePlan pl = plan_single<Op>(a.n, a.n);
     float4* tgt = ws.take<float4>((size_t)NT * pl.n_tpad);
@@ -367,9 +365,7 @@ int cov_run(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     return dispatch_kind_q(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, Q_ = decltype(deg)::value, D_ = decltype(D)::value;
-            if constexpr (sizeof(Real) == 4) {
-                if (a.n <= kSmallTargets) return cov_impl<Real, K_, Q_, D_, true>(a, ws, st);
-            }
+            if (a.n <= kSmallTargets) return cov_impl<Real, K_, Q_, D_, true>(a, ws, st);
             return cov_impl<Real, K_, Q_, D_>(a, ws, st);
         });
     });

@@ -80,13 +80,15 @@ def test_curve_norms_golden(golden, mods, precision, kname, err):
 
 @pytest.mark.parametrize("precision", ["fp32c", "fp64"])
 @pytest.mark.parametrize("err", ["current", "measure", "varifold"])
-def test_surface_norms_larger_mesh_against_oracle(oracle_lib, mods, precision, err):
-    """Subdivision-3 icosphere (642 vertices, 1280 faces) vs the oracle's numpy formulas."""
+@pytest.mark.parametrize("subdiv", [3, 4])
+def test_surface_norms_larger_mesh_against_oracle(oracle_lib, mods, precision, err, subdiv):
+    """Subdivision-3 / 4 icospheres (1280 / 5120 faces: the small and the large
+    tile shapes of the sweeps) vs the oracle's formulas."""
     from oracle import lddmm_ref as ref
     from registration_b200 import geometry as geo
     kf, sf, _ = mods
     rng = np.random.default_rng(17)
-    v, f = geo.icosphere(3)
+    v, f = geo.icosphere(subdiv)
     vt = geo.bumped_sphere(v, f, 8, 0.25, 0.15, rng)
     vd = v + 0.02 * rng.standard_normal(v.shape)
     K = kf.Kernel(name="gauss", sigma=0.1, precision=precision)
