@@ -54,7 +54,7 @@ OPS = [  # name, kernel, op, flops/pair, FMA-pipe instr/pair, XU ops/pair (per-p
 # bounding box (init, keys, finish), target / source packs (+1 target value pack for DKT), sweep, combine
 LAUNCHES_PER_OP = {"K": 7, "DKT": 8}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one sweep launch
-# at N = M = 2^20, from one ncu capture of this workload (profiles/sweep_kernels_1M_dram.md)
+# at N = M = 2^20, from one ncu metrics capture of this workload's sweep kernels
 TRAFFIC_1M = {"applyK_gauss": 87339264 + 89124864, "applyDiffKT_gauss": 148929024 + 94077952,
               "applyK_lap3": 88632576 + 84919296, "applyDiffKT_lap3": 170131712 + 133973760}
 
@@ -244,22 +244,40 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def _probe_lib():
+    """The issue-rate probe kernels (registration_b200/probe/liblddmm_probe.so,
+    a measurement utility outside the LDDMM library)."""
+    import ctypes
+    from registration_b200 import build as b
+    if not os.path.exists(b.PROBE_LIB):
+        b.build_probe()
+    L = ctypes.CDLL(b.PROBE_LIB)
+    L.lddmm_probe_launch.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_void_p]
+    L.lddmm_probe_launch.restype = ctypes.c_int
+    return L
+
+
 def measure_peaks(torch, lib, dev):
     """FP32 FMA and MUFU ex2 issue rates of this GPU (instr/s, all SMs)."""
-    from registration_b200 import _lib
     from registration_b200.device import ptr, stream_handle
+    P = _probe_lib()
+
+    def launch(what, blocks, threads, iters, out):
+        rc = P.lddmm_probe_launch(what, blocks, threads, iters, ptr(out), stream_handle())
+        if rc != 0:
+            raise RuntimeError("probe launch failed (%d)" % rc)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     blocks, threads = sms * 8, 256
     out = torch.empty(blocks * threads, dtype=torch.float32, device=dev)
     res = {}
     for what, iters in ((0, 20000), (1, 4000)):
         for _ in range(2):
-            _lib.call("lddmm_probe_launch", what, blocks, threads, iters, ptr(out), stream_handle())
+            launch(what, blocks, threads, iters, out)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         best = None
         for _ in range(3):
             e0.record()
-            _lib.call("lddmm_probe_launch", what, blocks, threads, iters, ptr(out), stream_handle())
+            launch(what, blocks, threads, iters, out)
             e1.record()
             e1.synchronize()
             t = e0.elapsed_time(e1) / 1e3

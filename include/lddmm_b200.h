@@ -335,14 +335,6 @@ LDDMM_API int lddmm_ragged_dataterm_f64(int nreq, int cell_size, int norm, const
                                         const int64_t* vertex_ptr, const int64_t* vertex_idx, double* px,
                                         void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
-/* ---- diagnostics ------------------------------------------------------------
- * No counterpart in the reference.  Launches `blocks` x `threads` threads that
- * each issue 8*iters FP32 FMAs (what = 0), 8*iters MUFU ex2 (what = 1) or
- * 8*iters packed two-lane FP32 FMAs (fma.rn.f32x2, what = 2) and
- * write one float to out[blocks*threads].  Timed by the benchmark to measure
- * the issue-rate peaks that the kernel-sum roofline is quoted against. */
-LDDMM_API int lddmm_probe_launch(int what, int blocks, int threads, int iters, float* out, lddmm_stream_t stream);
-
 #ifdef __cplusplus
 }
 #endif

@@ -493,7 +493,8 @@ def cg(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=10., trace=None
                 if (skipCG == 1) | (beta < 1e-10):
                     logging.info('Stopping Gradient Descent: bad direction')
                     break
-                else:
+                elif verb:
+                    # conjugateGradient.py:151-154: only under `if verb:`
                     skipCG = 1
                     noUpdate = 1
             else:

@@ -4,7 +4,9 @@
 
 Each .cu under registration_b200/csrc is compiled to an object (in parallel)
 and linked into registration_b200/liblddmm_b200.so.  Objects are rebuilt only
-when a source or header is newer.
+when a source or header is newer.  The issue-rate probe kernels that the
+benchmark measures its peaks with (registration_b200/probe/probe.cu) are a
+measurement utility, built into their own registration_b200/probe/liblddmm_probe.so.
 """
 import concurrent.futures as cf
 import glob
@@ -17,6 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblddmm_b200.so")
+PROBE_SRC = os.path.join(HERE, "probe", "probe.cu")
+PROBE_LIB = os.path.join(HERE, "probe", "liblddmm_probe.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -58,7 +62,21 @@ def build(verbose_ptxas=False, jobs=None):
         if HOSTCC:
             cmd += ["-ccbin", HOSTCC]
         subprocess.run(cmd, check=True)
+    build_probe()
     return LIB, logs
+
+
+def build_probe():
+    if os.path.exists(PROBE_LIB) and os.path.getmtime(PROBE_LIB) >= os.path.getmtime(PROBE_SRC):
+        return PROBE_LIB
+    cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
+                           "-fvisibility=hidden", "-shared", PROBE_SRC, "-o", PROBE_LIB, "-lcudart"]
+    if HOSTCC:
+        cmd += ["-ccbin", HOSTCC]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (PROBE_SRC, r.stdout, r.stderr))
+    return PROBE_LIB
 
 
 if __name__ == "__main__":

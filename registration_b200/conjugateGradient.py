@@ -86,10 +86,13 @@ def cg(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=10.):
                     logging.info('Stopping Gradient Descent: bad direction')
                     break
                 else:
+                    # conjugateGradient.py:151-154 disables CG and skips the
+                    # update only when verb is true; with verb false the
+                    # search goes on to the halving loop and accepts objTry
                     if verb:
                         logging.info('Disabling CG: bad direction')
-                    skipCG = 1
-                    noUpdate = 1
+                        skipCG = 1
+                        noUpdate = 1
             else:
                 while (objTry > obj) and (eps > epsMin):
                     eps = eps / 2

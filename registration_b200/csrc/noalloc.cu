@@ -70,6 +70,10 @@ extern "C" LDDMM_API int lddmm_applyk_f32c_noalloc(const double* x, int64_t n, c
                   (long long)n, (long long)m, d, dimb, sigma, order);
         return LDDMM_ERR_ARG;
     }
+    if (n > (1LL << 30) || m > (1LL << 30)) {   // the same limit as lddmm_applyk_f32c
+        set_error("applyk_noalloc: more than 2^30 points");
+        return LDDMM_ERR_ARG;
+    }
     int cap = 0;
     if (n > 0 && m > 0) {
         // largest chunk count whose workspace fits the static scratch

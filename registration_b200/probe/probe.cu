@@ -1,9 +1,16 @@
-// Diagnostic kernels that measure this GPU's FP32 FMA and MUFU ex2 issue rates.
-// bench.py times them to get the measured peaks that the kernel-sum roofline
-// fractions are quoted against.
-#include "host.h"
+// Measurement utility, not part of the LDDMM library: kernels that measure this
+// GPU's FP32 FMA, MUFU ex2 and packed f32x2 FMA issue rates.  bench.py times
+// them to get the measured peaks that the kernel-sum roofline fractions are
+// quoted against.  Built into its own liblddmm_probe.so.
+#include <cuda_runtime.h>
 
-namespace lddmm {
+namespace {
+
+__device__ __forceinline__ float ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
 // 8 independent FMA chains per thread, unrolled: 8*iters FFMA per thread.
 static __global__ void probe_ffma_kernel(float* out, int iters, float a, float b) {
@@ -60,16 +67,20 @@ static __global__ void probe_ffma2_kernel(float* out, int iters) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-}  // namespace lddmm
+}  // namespace
 
-extern "C" LDDMM_API int lddmm_probe_launch(int what, int blocks, int threads, int iters, float* out,
-                                            lddmm_stream_t stream) {
-    using namespace lddmm;
-    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || what < 0 || what > 2) {
-        set_error("probe: invalid launch (what=%d blocks=%d threads=%d iters=%d)", what, blocks, threads, iters);
-        return LDDMM_ERR_ARG;
+// Launches `blocks` x `threads` threads that each issue 8*iters FP32 FMAs
+// (what = 0), 8*iters MUFU ex2 (what = 1) or 8*iters packed two-lane FMAs
+// (what = 2) and write one float each to out[blocks*threads] (a device buffer).
+// Returns 0, -1 for a bad launch shape or a non-device `out`, -3 for a CUDA error.
+extern "C" __attribute__((visibility("default"))) int lddmm_probe_launch(int what, int blocks, int threads,
+                                                                         int iters, float* out, void* stream) {
+    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || what < 0 || what > 2) return -1;
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, out) != cudaSuccess || pa.type != cudaMemoryTypeDevice) {
+        cudaGetLastError();
+        return -1;
     }
-    LDDMM_TRY(check_device_ptr(out, "out"));
     cudaStream_t st = (cudaStream_t)stream;
     if (what == 0)
         probe_ffma_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999f, 1e-4f);
@@ -77,5 +88,5 @@ extern "C" LDDMM_API int lddmm_probe_launch(int what, int blocks, int threads, i
         probe_ex2_kernel<<<blocks, threads, 0, st>>>(out, iters);
     else
         probe_ffma2_kernel<<<blocks, threads, 0, st>>>(out, iters);
-    return cuda_check(cudaGetLastError(), "probe launch");
+    return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }

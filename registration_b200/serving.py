@@ -53,6 +53,14 @@ from .device import require_cuda
 NORMS = _rg.NORMS
 
 
+class RequestCancelled(Exception):
+    """A request withdrawn with MatchRequest.cancel()."""
+
+
+class ServingStopped(RuntimeError):
+    """The engine stopped (its run() left on an exception) before the request ended."""
+
+
 def _volume(v, f):
     """Signed volume sum_f det(v0, v1, v2) / 6 (surfaces.py:711-717)."""
     return float((np.linalg.det(v[f]) / 6).sum())
@@ -64,10 +72,16 @@ class MatchRequest:
     Template / Target: surfaces.Surface or curves.Curve (vertices, faces);
     param: SurfaceMatchingParam / CurveMatchingParam (timeStep, KparDiff,
     KparDist, sigmaError, errorType); maxIter / regWeight as in
-    SurfaceMatching.  The kernels' sigma / name / order are used; the kernel
-    sums run in FP32 with compensated accumulation whatever their precision."""
+    SurfaceMatching; verb is the matching classes' verb, passed to cg (it
+    selects cg's branch after a failed tiny step, conjugateGradient.py:151-154);
+    at_init: initial momenta (T, n, d), zero when None (SurfaceMatching starts
+    from zero, surfaceMatching.py:110).  cancel() withdraws the request: a
+    queued request is dropped, an active one stops at its next GPU call; both
+    end with a RequestCancelled error and free their slot and budget.
+    The kernels' sigma / name / order are used; the kernel sums run in FP32
+    with compensated accumulation whatever their precision."""
 
-    def __init__(self, Template, Target, param, maxIter=50, regWeight=1.0, rid=None):
+    def __init__(self, Template, Target, param, maxIter=50, regWeight=1.0, rid=None, verb=True, at_init=None):
         if param.errorType not in NORMS:
             raise ValueError("errorType must be one of %s" % sorted(NORMS))
         self.v0 = np.ascontiguousarray(np.asarray(Template.vertices, dtype=np.float64))
@@ -78,7 +92,8 @@ class MatchRequest:
             raise ValueError("template and target must have the same cell size and dimension")
         if param.errorType == "varifold" and self.f0.shape[1] != 3:
             raise ValueError("the varifold norm is defined for triangulated surfaces")
-        if self.f0.shape[1] == 3 and self.v0.shape[1] == 3:
+        if self.f0.shape[1] == 3 and self.v0.shape[1] == 3 and np.isfinite(self.v0).all() \
+                and np.isfinite(self.v1).all():
             # SurfaceMatching orients the target like the template (surfaceMatching.py:126-129)
             if _volume(self.v0, self.f0) * _volume(self.v1, self.f1) < 0:
                 self.f1 = np.ascontiguousarray(self.f1[:, [0, 2, 1]])
@@ -89,6 +104,13 @@ class MatchRequest:
         self.T = int(round(1.0 / param.timeStep))
         self.max_iter = int(maxIter)
         self.regweight = float(regWeight)
+        self.verb = bool(verb)
+        self.at_init = None
+        if at_init is not None:
+            self.at_init = np.ascontiguousarray(np.asarray(at_init, dtype=np.float64))
+            if self.at_init.shape != (self.T, len(self.v0), self.v0.shape[1]):
+                raise ValueError("at_init must be (T, n, d) = %s" % ((self.T, len(self.v0), self.v0.shape[1]),))
+        self.cancelled = False
         self.rid = rid
         self.arrival = None
         self.start = None
@@ -100,6 +122,22 @@ class MatchRequest:
     @property
     def n(self):
         return len(self.v0)
+
+    def cancel(self):
+        """Withdraws the request (see the class docstring)."""
+        self.cancelled = True
+
+    def input_error(self):
+        """ValueError for inputs no solve can start from (non-finite vertices or
+        initial momenta, cell indices out of range), else None."""
+        for name, a in (("template vertices", self.v0), ("target vertices", self.v1),
+                        ("initial momenta", self.at_init)):
+            if a is not None and not np.isfinite(a).all():
+                return ValueError("request %s: %s are not finite" % (self.rid, name))
+        for name, f, v in (("template", self.f0, self.v0), ("target", self.f1, self.v1)):
+            if f.size and (f.min() < 0 or f.max() >= len(v)):
+                return ValueError("request %s: %s cell indices out of range" % (self.rid, name))
+        return None
 
     @property
     def group(self):
@@ -155,7 +193,10 @@ class _Problem:
         self.noise_obs = 0.0
         self.dshape = _dt.DeviceShape(req.f0, req.n)
         self.tshape = _dt.DeviceShape(req.f1, len(req.v1))
-        self.at = torch.zeros((self.T, self.npt, self.dim), dtype=torch.float64, device=dev)
+        if req.at_init is None:
+            self.at = torch.zeros((self.T, self.npt, self.dim), dtype=torch.float64, device=dev)
+        else:
+            self.at = torch.from_numpy(req.at_init).to(dev)
         self.atTry = self.at
         self.xt = self.x0.unsqueeze(0).repeat(self.T + 1, 1, 1)
         self.xtTry = None
@@ -186,6 +227,11 @@ class _Problem:
         if self.obj is None:
             self.obj0 = self.engine.post(self, "norm0", None)
             self.obj, self.xt = self._value(self.at)
+            # the reference maps a NaN trial to 1e500 (surfaceMatching.py:278-280), which
+            # rejects that step; a non-finite starting objective has no step to reject
+            if not np.isfinite(float(self.obj)):
+                raise FloatingPointError("request %s: the objective at the initial momenta is not finite"
+                                         % self.req.rid)
         return self.obj
 
     def updateTry(self, dir, eps, objRef=None):
@@ -291,8 +337,12 @@ class Scheduler:
         return req
 
     def post(self, prob, kind, payload):
+        if getattr(prob.req, "cancelled", False):
+            raise RequestCancelled("request %s cancelled" % prob.req.rid)
         ev = threading.Event()
         with self.cv:
+            if self._stop:
+                raise ServingStopped("the engine has stopped")
             self.events[prob] = ev
             prob.lane.pending[prob] = (kind, payload)
             self.cv.notify_all()
@@ -300,6 +350,8 @@ class Scheduler:
         res = self.results.pop(prob)
         if isinstance(res, BaseException):
             raise res
+        if getattr(prob.req, "cancelled", False):
+            raise RequestCancelled("request %s cancelled" % prob.req.rid)
         return res
 
     def _run_request(self, req, lane, slot):
@@ -320,7 +372,7 @@ class Scheduler:
                 grd = prob.getGradient(prob.gradCoeff)
                 [g2] = prob.dotProduct(grd, [grd])
                 prob.gradEps = max(0.001, np.sqrt(g2) / 10000)
-                cg.cg(prob, verb=False, maxIter=req.max_iter, TestGradient=False,
+                cg.cg(prob, verb=getattr(req, "verb", True), maxIter=req.max_iter, TestGradient=False,
                       epsInit=getattr(req, "eps_init", 0.1))
                 obj = prob.obj.refine() if isinstance(prob.obj, _Value) else float(prob.obj)
                 req.result = {"at": prob.at, "xt": prob.xt, "obj": obj, "iters": prob.iters,
@@ -348,7 +400,15 @@ class Scheduler:
         with self.cv:
             keep = []
             for req in self.queue:
-                if req.arrival > now:
+                bad = RequestCancelled("request %s cancelled" % req.rid) if getattr(req, "cancelled", False) else None
+                if bad is None and req.arrival <= now and hasattr(req, "input_error"):
+                    bad = req.input_error()
+                if bad is not None:
+                    req.error = bad
+                    req.start = req.finish = now
+                    self.finished.append(req)
+                    req.done.set()
+                elif req.arrival > now:
                     keep.append(req)
                 elif req.hbm_bytes() > self.hbm_budget:
                     req.error = MemoryError("request needs %.3g bytes of device state; the budget is %.3g"
@@ -395,7 +455,11 @@ class Scheduler:
                     ready = lane.pending
                     lane.pending = {}
                 t0 = time.perf_counter()
-                self._execute(ready)
+                try:
+                    self._execute(ready)
+                except BaseException as exc:   # e.g. KeyboardInterrupt in a launch
+                    self._fail_waiting(ready, exc)
+                    raise
                 with self.stats_lock:
                     self.busy_seconds += time.perf_counter() - t0
                     self.rounds += 1
@@ -425,10 +489,33 @@ class Scheduler:
                 self.cv.notify_all()
             for lane in self.lanes:
                 lane.thread.join()
-            # every request thread has finished its work; let them exit
+            # on a normal exit every request has ended; after an exception, fail the
+            # requests still queued or waiting for a round so their threads end
+            with self.cv:
+                stopped = ServingStopped("the engine stopped before the request ended")
+                for req in self.queue:
+                    req.error = stopped
+                    req.finish = time.perf_counter()
+                    self.finished.append(req)
+                    req.done.set()
+                self.queue = []
+                waiting = {}
+                for lane in self.lanes:
+                    waiting.update(lane.pending)
+                    lane.pending = {}
+            self._fail_waiting(waiting, stopped)
             for th in self.threads:
                 th.join()
             self.threads = []
+
+    def _fail_waiting(self, items, exc):
+        """Hands `exc` to the request threads blocked in post() for `items`."""
+        with self.cv:
+            for prob in list(items):
+                ev = self.events.pop(prob, None)
+                if ev is not None:
+                    self.results[prob] = exc
+                    ev.set()
 
     def _execute(self, ready):
         groups = {}

@@ -4,8 +4,8 @@ The reference (saurabh-jain/registration, py-lddmm/) is Python 2 code over an
 f2py Fortran module.  In this container there is neither a Python 2
 interpreter nor a Fortran compiler, so this script:
 
-1. loads the reference's own Python modules from the read-only checkout
-   (default /root/reference/py-lddmm, or $LDDMM_REFERENCE_DIR) after four
+1. loads the reference's own Python modules from the read-only reference
+   checkout (its py-lddmm/ directory, or $LDDMM_REFERENCE_DIR) after four
    mechanical, semantics-preserving source rewrites done in memory
    (nothing is copied into this repository):
      - tabs expanded to 8-column stops (Python 2 indentation rule);

@@ -284,3 +284,116 @@ def test_match_request_orients_target_and_picks_the_protocol_step():
     c, _ = geo.ellipse_curve(32)
     rc = serving.MatchRequest(cv.Curve(pointSet=c), cv.Curve(pointSet=1.1 * c), P())
     assert rc.f0.shape[1] == 2 and rc.eps_init == 10.0
+
+
+class _CancellingEngine(_ToyEngine):
+    """Cancels request `victim` once it has taken `after` value launches."""
+
+    def __init__(self, victim, after, **kw):
+        super().__init__(**kw)
+        self.victim, self.after = victim, after
+
+    def _do_value(self, items):
+        for p, _ in items:
+            if p.req is self.victim and p.calls["value"] >= self.after:
+                self.victim.cancelled = True
+        return super()._do_value(items)
+
+
+def test_cancelled_requests_end_and_free_their_slot():
+    """A queued request cancelled before admission never starts; an active one
+    stops at its next GPU call.  Both end with RequestCancelled, give back their
+    slot and budget, and the others finish exactly as alone."""
+    reqs = [_ToyRequest(i, 6 + i, max_iter=60) for i in range(4)]
+    queued = _ToyRequest(9, 5)
+    queued.cancelled = True
+    eng = _CancellingEngine(reqs[1], after=3, max_active=4)
+    for r in reqs + [queued]:
+        eng.submit(r)
+    eng.run()
+    assert isinstance(queued.error, serving.RequestCancelled) and queued.start == queued.finish
+    assert isinstance(reqs[1].error, serving.RequestCancelled)
+    assert eng.n_active == 0 and eng.hbm_in_use == 0 and not eng.threads
+    assert eng.stats()["failed"] == 2
+    for r in (reqs[0], reqs[2], reqs[3]):
+        assert r.error is None and r.result["obj"] == _alone(r).result["obj"]
+
+
+class _BadInput(_ToyRequest):
+    def input_error(self):
+        return ValueError("request %s: target vertices are not finite" % self.rid)
+
+
+def test_invalid_inputs_fail_at_admission_others_served():
+    bad, good = _BadInput(0, 5), _ToyRequest(1, 7)
+    eng = _ToyEngine()
+    eng.submit(bad)
+    eng.submit(good)
+    eng.run()
+    assert isinstance(bad.error, ValueError) and bad.result is None
+    assert good.error is None and good.result["obj"] == _alone(good).result["obj"]
+
+
+class _InterruptedEngine(_ToyEngine):
+    """run() leaves on an exception while requests are waiting for rounds."""
+
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        self.values = 0
+
+    def _do_value(self, items):
+        self.values += 1
+        return super()._do_value(items)
+
+    def _can_admit(self, now):
+        if self.values >= 4:
+            raise KeyboardInterrupt
+        return super()._can_admit(now)
+
+
+def test_run_leaving_on_an_exception_ends_every_request_thread():
+    reqs = [_ToyRequest(i, 6, max_iter=500) for i in range(3)]
+    late = _ToyRequest(7, 6)
+    eng = _InterruptedEngine()
+    for r in reqs:
+        eng.submit(r)
+    eng.submit(late, arrival=time.perf_counter() + 3600.0)
+    done = threading.Event()
+    caught = []
+
+    def drive():
+        try:
+            eng.run()
+        except KeyboardInterrupt as exc:
+            caught.append(exc)
+        done.set()
+
+    th = threading.Thread(target=drive, daemon=True)
+    th.start()
+    assert done.wait(30.0), "run() did not return: request threads were left blocked"
+    assert caught and not eng.threads
+    for r in reqs + [late]:
+        assert r.done.is_set() and r.error is not None
+    assert isinstance(late.error, serving.ServingStopped)
+
+
+def test_match_request_input_checks():
+    from registration_b200 import geometry as geo
+    from registration_b200 import surfaces as sf
+
+    class P:
+        timeStep = 0.2
+        errorType = "varifold"
+    v, f = geo.icosphere(1)
+    ok = serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[f, 1.1 * v]), P())
+    assert ok.input_error() is None
+    vt = 1.1 * v
+    vt[3, 1] = np.nan
+    assert "target vertices" in str(serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[f, vt]),
+                                                         P()).input_error())
+    at = np.zeros((5, len(v), 3))
+    at[2, 0, 0] = np.inf
+    r = serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[f, 1.1 * v]), P(), at_init=at)
+    assert "initial momenta" in str(r.input_error())
+    with pytest.raises(ValueError):
+        serving.MatchRequest(sf.Surface(FV=[f, v]), sf.Surface(FV=[f, 1.1 * v]), P(), at_init=at[:2])

@@ -293,6 +293,50 @@ def test_serving_late_arrivals_and_hbm_budget_are_bit_identical():
     assert eng.stats()["max_active"] >= 2
 
 
+def test_faulty_and_cancelled_requests_fail_alone():
+    """A request with a NaN target vertex fails at admission; one whose initial
+    momenta overflow FP32 (1e200) gets a non-finite objective on the GPU and
+    fails with FloatingPointError; one cancelled after three value rounds ends
+    with RequestCancelled.  All three give back their slot and budget, and the
+    requests sharing their launches finish bit-identical to their solo runs."""
+    from registration_b200 import serving
+    from registration_b200 import surfaces as sf
+
+    good = _make_requests([0, 2])
+    victim = _make_requests([1])[0]
+    base = _make_requests([3])[0]
+    vt = base.v1.copy()
+    vt[5, 2] = np.nan
+    nan_target = serving.MatchRequest(sf.Surface(FV=[base.f0, base.v0]), sf.Surface(FV=[base.f1, vt]), base.param,
+                                      maxIter=8, rid="nan-target")
+    huge = serving.MatchRequest(sf.Surface(FV=[base.f0, base.v0]), sf.Surface(FV=[base.f1, base.v1]), base.param,
+                                maxIter=8, rid="overflow",
+                                at_init=np.full((base.T, base.n, 3), 1e200))
+
+    class Cancelling(serving.ServingEngine):
+        def _do_value(self, items):
+            for p, _ in items:
+                if p.req is victim and p.calls["value"] >= 3:
+                    victim.cancel()
+            return super()._do_value(items)
+
+    eng = Cancelling()
+    for r in good + [victim, nan_target, huge]:
+        eng.submit(r)
+    eng.run()
+    assert isinstance(nan_target.error, ValueError) and "not finite" in str(nan_target.error)
+    assert isinstance(huge.error, FloatingPointError)
+    assert isinstance(victim.error, serving.RequestCancelled)
+    st = eng.stats()
+    assert st["failed"] == 3 and st["finished"] == 5
+    assert eng.n_active == 0 and eng.hbm_in_use == 0
+    for r in good:
+        alone = _make_requests([r.rid])
+        serving.serve(alone)
+        a, b = _result(alone[0]), _result(r)
+        assert a["obj"] == b["obj"] and a["iters"] == b["iters"] and torch.equal(a["at"], b["at"])
+
+
 def test_serving_rejects_requests_above_the_budget():
     from registration_b200 import serving
     reqs = _make_requests([0, 2], iters=2)
@@ -313,7 +357,7 @@ def test_serving_matches_single_problem_driver():
     serving.serve(reqs)
     for r in reqs:
         sm = SurfaceMatching(Template=sf.Surface(FV=[r.f0, r.v0]), Target=sf.Surface(FV=[r.f1, r.v1]),
-                             param=r.param, maxIter=10, regWeight=1.0, verb=False, testGradient=False,
+                             param=r.param, maxIter=10, regWeight=1.0, verb=r.verb, testGradient=False,
                              lineSearchPrecision="fp64")
         sm.optimizeMatching()
         res = _result(r)
