@@ -351,6 +351,42 @@ def varifoldNormGradient(fvDef, fv1, KparDist):
     return _scatter3(fvDef, dz1, z1)
 
 
+# The same three varifold functions with the F x F weights formed per pair in
+# C (oracle.varifold_pairs) instead of as dense arrays, for face counts whose
+# F x F x 3 FP64 temporaries do not fit in host memory (about 10 GB per array
+# at 20,480 faces).  The sums are linear in the source weights a_l, so the
+# S1 and S2 terms of surfaces.py:1200-1276 are one call over the stacked
+# sources [c1; c2] with signed weights.
+def _pair_sources(fvA, fvB, wB):
+    a1, a2, n1, n2 = _varifold_terms(fvA.centers, fvA.surfel, fvB.centers, fvB.surfel)
+    if fvB is fvA:
+        return fvA.centers, n1, a1, fvA.centers, n1, a1
+    return (fvA.centers, n1, a1, np.vstack([fvA.centers, fvB.centers]), np.vstack([n1, n2]),
+            np.concatenate([a1, wB * a2]))
+
+
+def varifoldNorm0_pairs(fv1, KparDist):
+    """varifoldNorm0 (surfaces.py:1184-1196) per pair."""
+    c1, n1, a1, c, n, a = _pair_sources(fv1, fv1, 1.0)
+    val, _, _ = _o.varifold_pairs(c1, n1, a1, c, n, a, KparDist.sigma, KparDist.order, want=("val",))
+    return float(val.sum())
+
+
+def varifoldNormDef_pairs(fvDef, fv1, KparDist):
+    """varifoldNormDef (surfaces.py:1200-1221) per pair: <S1,S1> - 2 <S1,S2>."""
+    c1, n1, a1, c, n, a = _pair_sources(fvDef, fv1, -2.0)
+    val, _, _ = _o.varifold_pairs(c1, n1, a1, c, n, a, KparDist.sigma, KparDist.order, want=("val",))
+    return float(val.sum())
+
+
+def varifoldNormGradient_pairs(fvDef, fv1, KparDist):
+    """varifoldNormGradient (surfaces.py:1228-1276) per pair: z1 = K u1 - K u2,
+    dz1 = (K'beta1 - K'beta2) / 3, then the vertex scatter."""
+    c1, n1, a1, c, n, a = _pair_sources(fvDef, fv1, -1.0)
+    _, z1, dz = _o.varifold_pairs(c1, n1, a1, c, n, a, KparDist.sigma, KparDist.order, want=("z", "dz"))
+    return _scatter3(fvDef, (1. / 3.) * dz, z1)
+
+
 # ---------------------------------------------------------------------------
 # Curves (py-lddmm/curves.py)
 # ---------------------------------------------------------------------------
@@ -681,7 +717,9 @@ class MatchingParam:
 class SurfaceMatching(_MatchingBase):
     """surfaceMatching.py:74-484 with affine='none', symmetric=False, no file output."""
 
-    def __init__(self, Template, Target, param, maxIter=1000, regWeight=1.0, testGradient=False, seed=0):
+    def __init__(self, Template, Target, param, maxIter=1000, regWeight=1.0, testGradient=False, seed=0,
+                 verb=True):
+        self.verb = verb
         self.fv0 = Surface(surf=Template)
         self.fv1 = Surface(surf=Target)
         self.param = param
@@ -713,14 +751,15 @@ class SurfaceMatching(_MatchingBase):
         grd = self.getGradient(self.gradCoeff)
         [grd2] = self.dotProduct(grd, [grd])
         self.gradEps = max(0.001, np.sqrt(grd2) / 10000)
-        cg(self, verb=False, maxIter=self.maxIter, TestGradient=self.testGradient, epsInit=0.1, trace=trace)
+        cg(self, verb=self.verb, maxIter=self.maxIter, TestGradient=self.testGradient, epsInit=0.1, trace=trace)
 
 
 class CurveMatching(_MatchingBase):
     """curveMatching.py:58-352 with affine='none', no file output."""
 
     def __init__(self, Template, Target, param, maxIter=1000, regWeight=1.0, gradLB=0.001, testGradient=False,
-                 seed=0):
+                 seed=0, verb=True):
+        self.verb = verb
         self.fv0 = Curve(curve=Template)
         self.fv1 = Curve(curve=Target)
         self.param = param
@@ -751,9 +790,9 @@ class CurveMatching(_MatchingBase):
         [grd2] = self.dotProduct(grd, [grd])
         self.gradEps = max(self.gradLB, np.sqrt(grd2) / 10000)
         if optimizer == 'cg':
-            cg(self, verb=False, maxIter=self.maxIter, TestGradient=self.testGradient, trace=trace)
+            cg(self, verb=self.verb, maxIter=self.maxIter, TestGradient=self.testGradient, trace=trace)
         else:
-            descend(self, verb=False, maxIter=self.maxIter, trace=trace)
+            descend(self, verb=self.verb, maxIter=self.maxIter, trace=trace)
 
 
 # ---------------------------------------------------------------------------
@@ -780,7 +819,8 @@ class SurfaceTemplate:
     are the x0 of the prior shot here, and no velocity is stored."""
 
     def __init__(self, HyperTmpl, Targets, param, maxIter=1000, lambdaPrior=1.0, regWeight=1.0, testGradient=True,
-                 seed=0):
+                 seed=0, verb=True):
+        self.verb = verb
         self.fv0 = Surface(surf=HyperTmpl)
         self.fv1 = [Surface(surf=ff) for ff in Targets]
         self.Ntarg = len(self.fv1)
@@ -937,5 +977,5 @@ class SurfaceTemplate:
         grd = self.getGradient(self.gradCoeff)
         [grd2] = self.dotProduct(grd, [grd])
         self.gradEps = max(0.1, np.sqrt(grd2) / 10000)
-        cg(self, verb=False, maxIter=self.maxIter, TestGradient=self.testGradient, trace=trace)
+        cg(self, verb=self.verb, maxIter=self.maxIter, TestGradient=self.testGradient, trace=trace)
         return self

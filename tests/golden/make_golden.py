@@ -27,7 +27,8 @@ interpreter nor a Fortran compiler, so this script:
 VTK writers are replaced by no-ops (output only; they do not change the
 optimisation state).  Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # both fixture files
+    python tests/golden/make_golden.py --kff-calls  # tests/golden/kff_calls.npz only
 """
 import io
 import os
@@ -447,10 +448,92 @@ def mesh_cases(R, out):
     out["mesh_off_f"] = back.faces
 
 
+class _KffRecorder:
+    """Stands in for the module ``kernelFunctions_fort`` of the reference's
+    kernelFunctions.py and records every call it receives (routine name, the
+    positional arguments exactly as the reference passes them, the result of
+    the oracle), at most `cap` calls per routine."""
+
+    def __init__(self, inner, cap=12):
+        self.inner, self.cap, self.calls, self.count = inner, cap, [], {}
+
+    def __getattr__(self, name):
+        fn = getattr(self.inner, name)
+
+        def call(*args):
+            res = fn(*args)
+            if self.count.get(name, 0) < self.cap:
+                self.count[name] = self.count.get(name, 0) + 1
+                self.calls.append((name, [np.array(a, copy=True) for a in args], np.array(res, copy=True)))
+            return res
+        return call
+
+
+def kff_call_cases(R):
+    """The calls the reference's own Python makes into kernelFunctions_fort
+    (Kernel.applyK / applyDiffKT / applyDiffKmat / applyDiffK*, through
+    landmarkHamiltonianGradient, the surface varifold and current gradients and
+    the curve current gradient), with the oracle's results, for replaying them
+    through a drop-in module."""
+    kf = R["kernelFunctions"]
+    ev = R["pointEvolution"]
+    sf = R["surfaces"]
+    cv = R["curves"]
+    rec = _KffRecorder(oracle.FortShim())
+    saved = kf.kff
+    kf.kff = rec
+    try:
+        rng = np.random.default_rng(99)
+        x, y = rng.uniform(0, 1, (40, 3)), rng.uniform(0, 1, (55, 3))
+        for K in (kf.Kernel(name="gauss", sigma=0.3), kf.Kernel(name="laplacian", sigma=0.3, order=2)):
+            K.applyK(y, rng.standard_normal((55, 3)))
+            K.applyK(y, rng.standard_normal((55, 1)), firstVar=x)
+            K.applyDiffKT(y, rng.standard_normal((1, 40, 3)), rng.standard_normal((1, 55, 3)), firstVar=x)
+            K.applyDiffK(x, rng.standard_normal((40, 3)), rng.standard_normal((40, 3)))
+            K.applyDiffK2(x, rng.standard_normal((40, 3)), rng.standard_normal((40, 3)))
+            K.applyDiffK1and2(x, rng.standard_normal((40, 3)), rng.standard_normal((40, 3)))
+            K.applyDDiffK11and12(x, rng.standard_normal((40, 3)), rng.standard_normal((40, 3)),
+                                 rng.standard_normal((40, 3)))
+        K = kf.Kernel(name="gauss", sigma=0.5)
+        x0 = rng.uniform(-1, 1, (30, 3))
+        ev.landmarkHamiltonianGradient(x0, 0.2 * rng.standard_normal((3, 30, 3)), rng.standard_normal((30, 3)), K,
+                                       1.0)
+        v, f = geo.icosphere(1)
+        vt = geo.bumped_sphere(v, f, 3, 0.4, 0.1, rng)
+        a, b = sf.Surface(FV=[f, v + 0.02 * rng.standard_normal(v.shape)]), sf.Surface(FV=[f, vt])
+        KD = kf.Kernel(name="gauss", sigma=0.4)
+        sf.varifoldNormGradient(a, b, KD)
+        sf.currentNormGradient(a, b, KD)
+        c, _ = geo.ellipse_curve(24)
+        ct, _ = geo.bumped_curve(c, 2, 0.3, 0.1, rng)
+        cv.currentNormGradient(cv.Curve(pointSet=c), cv.Curve(pointSet=ct), kf.Kernel(name="laplacian", sigma=0.5,
+                                                                                       order=3))
+    finally:
+        kf.kff = saved
+    out = {"ncalls": np.array(len(rec.calls))}
+    for i, (name, args, res) in enumerate(rec.calls):
+        out["c%d_name" % i] = np.array(name)
+        out["c%d_nargs" % i] = np.array(len(args))
+        for j, a in enumerate(args):
+            out["c%d_a%d" % (i, j)] = a
+        out["c%d_out" % i] = res
+    return out
+
+
+def write_kff_calls(R):
+    calls = kff_call_cases(R)
+    dst = os.path.join(HERE, "kff_calls.npz")
+    np.savez_compressed(dst, **calls)
+    print("wrote %s (%d calls, %.1f KB)" % (dst, int(calls["ncalls"]), os.path.getsize(dst) / 1024.0))
+
+
 def main():
     oracle.build()
     oracle.set_num_threads(4)
     R = load_reference()
+    if "--kff-calls" in sys.argv:     # only the recorded kernelFunctions_fort calls
+        write_kff_calls(R)
+        return
     out = {}
     kernel_cases(R, out)
     second_cases(R, out)
@@ -464,6 +547,7 @@ def main():
     dst = os.path.join(HERE, "reference_golden.npz")
     np.savez_compressed(dst, **out)
     print("wrote %s (%d arrays, %.1f KB)" % (dst, len(out), os.path.getsize(dst) / 1024.0))
+    write_kff_calls(R)
 
 
 if __name__ == "__main__":

@@ -205,3 +205,19 @@ def test_template_estimation_trace_matches_reference(golden, oracle_lib, err, la
     np.testing.assert_allclose(st.at, golden[p + "at"], rtol=1e-7, atol=1e-10)
     np.testing.assert_allclose(np.stack(st.atAll), golden[p + "atAll"], rtol=1e-7, atol=1e-10)
     np.testing.assert_allclose(st.fvTmpl.vertices, golden[p + "tmpl"], rtol=1e-9, atol=1e-12)
+
+
+def test_per_pair_varifold_equals_dense_varifold(oracle_lib):
+    """The per-pair varifold functions (for face counts whose F x F arrays do
+    not fit) against the dense restatement of surfaces.py:1184-1276."""
+    from registration_b200 import geometry as geo
+    rng = np.random.default_rng(4)
+    v, f = geo.icosphere(2)
+    vt = geo.bumped_sphere(v, f, 4, 0.3, 0.1, rng)
+    vd = v + 0.03 * rng.standard_normal(v.shape)
+    K = ref.Kernel(name="gauss", sigma=0.2)
+    a, b = ref.Surface(FV=[f, vd]), ref.Surface(FV=[f, vt])
+    n0 = abs(ref.varifoldNorm0(b, K))
+    assert abs(ref.varifoldNorm0_pairs(b, K) - ref.varifoldNorm0(b, K)) < 1e-12 * n0
+    assert abs(ref.varifoldNormDef_pairs(a, b, K) - ref.varifoldNormDef(a, b, K)) < 1e-12 * n0
+    assert _rel(ref.varifoldNormGradient_pairs(a, b, K), ref.varifoldNormGradient(a, b, K)) < 1e-12
