@@ -78,6 +78,12 @@ def parse():
     ap.add_argument("--max-active", type=int, default=64, help="serving slots")
     ap.add_argument("--line-search", default="auto", choices=["auto", "fp64", "fp32c"],
                     help="precision of the data-term values compared by the served line search")
+    ap.add_argument("--baseline", default="fit", choices=["fit", "measured"],
+                    help="serving workload: one-at-a-time baselines fitted from six requests or measured on all")
+    ap.add_argument("--serve-requests", type=int, default=16,
+                    help="requests of the short served stream reported beside the kernel-sum line (0: none)")
+    ap.add_argument("--no-matching", action="store_true",
+                    help="kernel-sum line without the surface-matching and served-matching records")
     ap.add_argument("--lanes", default="5000,16000",
                     help="serving size-class bounds (vertex counts), comma separated, or 'none'")
     return ap.parse_args()
@@ -408,18 +414,16 @@ def run_curve(args):
     return 0
 
 
-def run_surface(args):
-    import logging
-    logging.disable(logging.INFO)
-    iters = args.iters or 100
-    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
-    v, f, vt = surface_problem()
-    config = {"workload": "surface matching: icosphere %d vertices / %d faces, 8 bumps, gauss sigma 0.2, varifold "
-                          "sigma 0.1, sigmaError %g, T 10, %d cg iterations" % (len(v), len(f), sig_err, iters)}
+def surface_measure(iters, sig_err, steps, with_ls64=True):
+    """The surface-matching workload (icosphere subdivision 5, 8 bumps, gauss
+    sigma 0.2, varifold sigma 0.1, T 10): FP32c kernel sums with the 'auto'
+    line search, timed `steps` times after a short warm-up, then FP32c with FP64
+    line-search values and the plain FP64 GPU path, once each."""
     import torch
     from registration_b200 import kernelFunctions as kf
     from registration_b200 import surfaceMatching as SM
     from registration_b200 import surfaces as sf
+    v, f, vt = surface_problem()
 
     def match(precision, maxit, lsp=None):
         param = SM.SurfaceMatchingParam(timeStep=0.1,
@@ -440,22 +444,73 @@ def run_surface(args):
     # FP32c with FP64 line-search values and plain FP64
     match("fp32c", 3)   # warm-up (library load, workspaces)
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         dt_, sm = match("fp32c", iters)
         times.append(dt_)
-    t_ls64, sm_ls64 = match("fp32c", iters, "fp64")
+    t_ls64, sm_ls64 = match("fp32c", iters, "fp64") if with_ls64 else (None, None)
     t64, sm64 = match("fp64", iters)
+    return {"v": v, "f": f, "vt": vt, "times": times, "sm": sm, "t_ls64": t_ls64, "sm_ls64": sm_ls64,
+            "t64": t64, "sm64": sm64}
+
+
+def surface_summary(m, sig_err, iters):
+    """The keys of the surface-matching record."""
+    sm, sm64 = m["sm"], m["sm64"]
+    val = 1.0 / float(np.mean(m["times"]))
+    return {"workload": "surface matching: icosphere %d vertices / %d faces, 8 bumps, gauss sigma 0.2, varifold "
+                        "sigma 0.1, sigmaError %g, T 10, at most %d cg iterations"
+                        % (len(m["v"]), len(m["f"]), sig_err, iters),
+            "matches_per_s": val, "line_search": "auto", "ms_per_match": 1e3 * float(np.mean(m["times"])),
+            "iterations": sm.iter, "final_energy": float(sm.obj), "calls": sm.calls,
+            "fp64_gpu": {"matches_per_s": 1.0 / m["t64"], "iterations": sm64.iter, "final_energy": float(sm64.obj)},
+            "fp32c_with_fp64_line_search": None if m["sm_ls64"] is None else
+            {"matches_per_s": 1.0 / m["t_ls64"], "iterations": m["sm_ls64"].iter,
+             "final_energy": float(m["sm_ls64"].obj)},
+            "speedup_vs_fp64_gpu": m["t64"] / float(np.mean(m["times"]))}
+
+
+def matching_records(args):
+    """The metric's matching clause beside the kernel-sum line: the surface
+    workload (sigmaError 0.01, at most 100 cg iterations; 'auto' line search
+    and the plain FP64 GPU path) and a short served stream of
+    --serve-requests requests (sigmaError 0.01, at most 50 iterations each)
+    with both one-at-a-time baselines measured on every request."""
+    import logging
+    logging.disable(logging.INFO)
+    try:
+        sig_err, iters = 0.01, 100
+        surf = surface_summary(surface_measure(iters, sig_err, steps=1, with_ls64=False), sig_err, iters)
+        served = None
+        if args.serve_requests > 0:
+            ekw = {"max_active": 64, "lanes": (5000, 16000), "line_search_precision": "auto"}
+            m = serving_measure(args.serve_requests, args.seed, 50, sig_err, ekw, "measured")
+            served = serving_summary(m, args.serve_requests, 50, sig_err, ekw)
+    finally:
+        logging.disable(logging.NOTSET)
+    return surf, served
+
+
+def run_surface(args):
+    import logging
+    logging.disable(logging.INFO)
+    iters = args.iters or 100
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
+    m = surface_measure(iters, sig_err, args.steps)
+    v, f, vt, sm, sm64 = m["v"], m["f"], m["vt"], m["sm"], m["sm64"]
+    config = {"workload": "surface matching: icosphere %d vertices / %d faces, 8 bumps, gauss sigma 0.2, varifold "
+                          "sigma 0.1, sigmaError %g, T 10, %d cg iterations" % (len(v), len(f), sig_err, iters)}
     cpu = None
     if not args.no_cpu_baseline:
         cpu = surface_cpu_estimate(v, f, vt, sm.calls)
+    times = m["times"]
     val = 1.0 / float(np.mean(times))
     _line(args, "surface matches/s", val, "matches/s", True, config,
           {"ms_per_step": 1e3 * float(np.mean(times)), "ms_per_iteration": 1e3 * float(np.mean(times)) / max(1, sm.iter),
            "final_energy_fp32c": sm.obj, "final_energy_fp64": sm64.obj,
            "final_energy_abs_diff": abs(sm.obj - sm64.obj), "iterations": sm.iter, "iterations_fp64": sm64.iter,
-           "fp64_gpu_ms": 1e3 * t64, "calls": sm.calls,
-           "fp32c_with_fp64_line_search": {"ms": 1e3 * t_ls64, "final_energy": sm_ls64.obj,
-                                           "iterations": sm_ls64.iter},
+           "fp64_gpu_ms": 1e3 * m["t64"], "calls": sm.calls,
+           "fp32c_with_fp64_line_search": {"ms": 1e3 * m["t_ls64"], "final_energy": m["sm_ls64"].obj,
+                                           "iterations": m["sm_ls64"].iter},
            "cpu_baseline": cpu,
            "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": int(v.nbytes + vt.nbytes + f.nbytes),
                    "d2h_bytes_per_step": int(sm.at.numel() * 8)}})
@@ -712,35 +767,57 @@ def _fresh(reqs):
                                  maxIter=r.max_iter, rid=r.rid) for r in reqs]
 
 
-def run_serving(args):
+def _one_at_a_time(r, maxit, mode):
+    """One request solved alone: 'fp64' = the plain FP64 single-problem GPU
+    driver (SurfaceMatching, FP64 kernels, FP64 line search), 'engine' = this
+    engine serving it as its only request (FP32c kernels, its line search).
+    Returns (seconds, iterations)."""
+    import torch
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import serving
+    from registration_b200 import surfaceMatching as SM
+    from registration_b200 import surfaces as sf
+    p = r.param
+    torch.cuda.synchronize()
+    ta = time.perf_counter()
+    if mode == "fp64":
+        param = SM.SurfaceMatchingParam(
+            timeStep=p.timeStep, KparDiff=kf.Kernel(name="gauss", sigma=p.KparDiff.sigma, precision="fp64"),
+            KparDist=kf.Kernel(name="gauss", sigma=p.KparDist.sigma, precision="fp64"),
+            sigmaError=p.sigmaError, errorType=p.errorType)
+        sm = SM.SurfaceMatching(Template=sf.Surface(FV=[r.f0, r.v0]), Target=sf.Surface(FV=[r.f1, r.v1]),
+                                param=param, maxIter=maxit, testGradient=False, verb=r.verb,
+                                lineSearchPrecision="fp64")
+        sm.optimizeMatching()
+        its = sm.iter
+    else:
+        q = _fresh([r])[0]
+        q.max_iter = maxit
+        serving.serve([q], max_active=1)
+        its = q.result["iters"]
+    torch.cuda.synchronize()
+    return time.perf_counter() - ta, its
+
+
+def serving_measure(R, seed, iters, sig_err, ekw, baseline="measured"):
     """Continuous batching of the request stream on one GPU.
 
     1. capacity: the first min(64, R) requests served closed-loop (all at t=0);
     2. the R-request stream with Poisson arrivals at 80% of that capacity:
        throughput = R / (last finish - first arrival), latency = finish - arrival;
-    3. one-at-a-time FP64 GPU solves (SurfaceMatching, FP64 kernels, FP64
-       line search) of six requests spread over the size range, a few cg
-       iterations each: per-iteration time fitted as a + b V^2 and summed over
+    3. the one-at-a-time baselines.  baseline='measured': every request of the
+       stream solved alone, one after the other, by the plain FP64 GPU driver
+       and by this engine; the stream's one-at-a-time throughput is R over the
+       summed times.  baseline='fit' (long streams): six requests spread over
+       the size range, per-iteration time fitted as a + b V^2 and summed over
        the stream with the served run's own iteration counts."""
-    import logging
-    logging.disable(logging.INFO)
     import torch
     from registration_b200 import serving
-    iters = args.iters or 50
-    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
-    R = args.requests
-    lanes = () if args.lanes in ("", "none") else tuple(int(b) for b in args.lanes.split(","))
-    ekw = {"max_active": args.max_active, "lanes": lanes, "line_search_precision": args.line_search}
     t_prep = time.perf_counter()
-    stream = serving_stream(R, args.seed, iters, sig_err)
+    stream = serving_stream(R, seed, iters, sig_err)
     t_prep = time.perf_counter() - t_prep
     sizes = np.array([r.n for r in stream])
-    config = {"workload": "served surface matching: %d requests, V ~ logU[2000, 50000] icosphere-derived, 4-16 "
-                          "bumps, gauss sigma ~ U[0.05, 0.3], varifold sigma = sigma/2, sigmaError %g, T 10, %d cg "
-                          "iterations max, Poisson arrivals at 80%% of measured capacity, %d slots, 150 GB HBM "
-                          "budget, size lanes %s, line search %s" % (R, sig_err, iters, args.max_active, list(lanes),
-                                                                     args.line_search)}
-    # warm-up: library load, workspace growth, cuBLAS handles
+    # warm-up: library load, workspace growth
     warm = _fresh([stream[int(np.argmin(sizes))]])
     for r in warm:
         r.max_iter = 2
@@ -755,7 +832,7 @@ def run_serving(args):
     cap = ncal / (time.perf_counter() - t0)
     # 2. open loop at 80% of capacity
     reqs = _fresh(stream)
-    rng = np.random.default_rng(args.seed + 1)
+    rng = np.random.default_rng(seed + 1)
     gaps = rng.exponential(1.0 / (0.8 * cap), size=R)
     clocks = ClockSampler(gpu_id_for(0))
     clocks.start()
@@ -773,59 +850,40 @@ def run_serving(args):
     lat = np.array([r.latency() for r in ok])
     its = np.array([r.result["iters"] for r in ok])
     thr = len(ok) / span
-    pred = pred32 = base_thr = None
-    coef_it = coef_set = coef_it32 = coef_set32 = None
-    samples = []
-    order = np.argsort(sizes)
-    if not args.no_fp64:
-        # 3. one-at-a-time solves of six requests across the size range: the plain
-        #    FP64 GPU driver (SurfaceMatching, FP64 kernels, FP64 line search), and
-        #    this engine serving one request alone (FP32c, no batching)
-        from registration_b200 import kernelFunctions as kf
-        from registration_b200 import surfaceMatching as SM
-        from registration_b200 import surfaces as sf
+    it_by_rid = {r.rid: r.result["iters"] for r in ok}
+    out = {"stream": stream, "ok": ok, "sizes": sizes, "thr": thr, "span": span, "cap": cap, "lat": lat,
+           "its": its, "stats": st, "clocks": clk, "prep_seconds": t_prep, "baseline": baseline}
+    if baseline == "measured":
+        _one_at_a_time(warm[0], 1, "fp64")    # warm-up of the FP64 driver
+        per = []
+        for r in stream:
+            t64, i64 = _one_at_a_time(r, iters, "fp64")
+            t32, i32 = _one_at_a_time(r, iters, "engine")
+            per.append({"V": int(r.n), "fp64_s": t64, "fp64_iters": int(i64), "engine_alone_s": t32,
+                        "engine_alone_iters": int(i32), "served_iters": int(it_by_rid.get(r.rid, -1))})
+        out["per_request"] = per
+        out["fp64_seconds"] = sum(q["fp64_s"] for q in per)
+        out["engine_alone_seconds"] = sum(q["engine_alone_s"] for q in per)
+        out["fit"] = None
+    elif baseline == "fit":
+        order = np.argsort(sizes)
         pick = [int(order[int(q * (R - 1))]) for q in (0.0, 0.2, 0.4, 0.6, 0.8, 1.0)]
         base_it = 4
         samples = []
         for idx in pick:
             r = stream[idx]
-            p = r.param
 
-            def solve(maxit):
-                param = SM.SurfaceMatchingParam(
-                    timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=p.KparDiff.sigma, precision="fp64"),
-                    KparDist=kf.Kernel(name="gauss", sigma=p.KparDist.sigma, precision="fp64"),
-                    sigmaError=p.sigmaError, errorType="varifold")
-                sm = SM.SurfaceMatching(Template=sf.Surface(FV=[r.f0, r.v0]), Target=sf.Surface(FV=[r.f1, r.v1]),
-                                        param=param, maxIter=maxit, testGradient=False, verb=False,
-                                        lineSearchPrecision="fp64")
-                torch.cuda.synchronize()
-                ta = time.perf_counter()
-                sm.optimizeMatching()
-                torch.cuda.synchronize()
-                return time.perf_counter() - ta, sm.iter
-
-            def alone(maxit):
-                q = _fresh([r])[0]
-                q.max_iter = maxit
-                torch.cuda.synchronize()
-                ta = time.perf_counter()
-                serving.serve([q], max_active=1)
-                torch.cuda.synchronize()
-                return time.perf_counter() - ta, q.result["iters"]
-
-            def two_point(fn):
-                fn(1)   # warm-up: workspaces, first-touch
-                t1, i1 = fn(1)
-                tk, ik = fn(base_it)
-                per = (tk - t1) / (ik - i1) if ik > i1 else tk / max(1, ik)
+            def two_point(mode):
+                _one_at_a_time(r, 1, mode)   # warm-up: workspaces, first-touch
+                t1, i1 = _one_at_a_time(r, 1, mode)
+                tk, ik = _one_at_a_time(r, base_it, mode)
+                per_it = (tk - t1) / (ik - i1) if ik > i1 else tk / max(1, ik)
                 return {"seconds_1": t1, "iters_1": int(i1), "seconds_k": tk, "iters_k": int(ik),
-                        "seconds_per_iter": per, "setup_seconds": max(0.0, t1 - i1 * per)}
-
-            samples.append({"V": int(r.n), "fp64_one_at_a_time": two_point(solve), "fp32c_alone": two_point(alone)})
+                        "seconds_per_iter": per_it, "setup_seconds": max(0.0, t1 - i1 * per_it)}
+            samples.append({"V": int(r.n), "fp64_one_at_a_time": two_point("fp64"),
+                            "fp32c_alone": two_point("engine")})
         Vs = np.array([s_["V"] for s_ in samples], dtype=np.float64)
         A = np.stack([np.ones_like(Vs), Vs ** 2], axis=1)
-        it_by_rid = {r.rid: r.result["iters"] for r in ok}
 
         def stream_seconds(key):
             c_it, *_ = np.linalg.lstsq(A, np.array([s_[key]["seconds_per_iter"] for s_ in samples]), rcond=None)
@@ -834,14 +892,62 @@ def run_serving(args):
                       + max(1, it_by_rid.get(r.rid, iters)) * max(0.0, c_it[0] + c_it[1] * n ** 2)
                       for r, n in zip(stream, sizes))
             return tot, [float(c_) for c_ in c_it], [float(c_) for c_ in c_set]
+        out["fp64_seconds"], c64, s64 = stream_seconds("fp64_one_at_a_time")
+        out["engine_alone_seconds"], c32, s32 = stream_seconds("fp32c_alone")
+        out["fit"] = {"samples": samples, "fp64_per_iter_fit_s": c64, "fp64_setup_fit_s": s64,
+                      "engine_per_iter_fit_s": c32, "engine_setup_fit_s": s32}
+        out["per_request"] = None
+    else:
+        out["fp64_seconds"] = out["engine_alone_seconds"] = None
+        out["per_request"] = out["fit"] = None
+    return out
 
-        pred, coef_it, coef_set = stream_seconds("fp64_one_at_a_time")
-        pred32, coef_it32, coef_set32 = stream_seconds("fp32c_alone")
-        base_thr = R / pred
+
+def serving_summary(m, R, iters, sig_err, ekw):
+    """The keys of the served-matching record."""
+    st, lat, its, sizes, ok = m["stats"], m["lat"], m["its"], m["sizes"], m["ok"]
+    base = R / m["fp64_seconds"] if m["fp64_seconds"] else None
+    alone = R / m["engine_alone_seconds"] if m["engine_alone_seconds"] else None
+    lanes = list(ekw.get("lanes", ()))
+    return {"workload": "served surface matching: %d requests, V ~ logU[2000, 50000] icosphere-derived, 4-16 "
+                        "bumps, gauss sigma ~ U[0.05, 0.3], varifold sigma = sigma/2, sigmaError %g, T 10, %d cg "
+                        "iterations max, Poisson arrivals at 80%% of measured capacity, %d slots, 150 GB HBM budget, "
+                        "size lanes %s, line search %s" % (R, sig_err, iters, ekw.get("max_active", 64), lanes,
+                                                          ekw.get("line_search_precision", "auto")),
+            "matches_per_s": m["thr"], "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "p99_ms": 1e3 * float(np.percentile(lat, 99)), "capacity_closed_loop": m["cap"],
+            "offered_rate": 0.8 * m["cap"], "span_s": m["span"], "failed": st["failed"], "rounds": st["rounds"],
+            "mean_batch": st["mean_batch"], "max_batch": st["max_batch"], "max_active": st["max_active"],
+            "lane_rounds": st["lane_rounds"], "iterations_mean": float(its.mean()), "iterations_min": int(its.min()),
+            "value_refinements": int(sum(r.result["calls"].get("refine", 0) for r in ok)),
+            "values": int(sum(r.result["calls"]["value"] for r in ok)),
+            "converged": int(sum(r.result["converged"] for r in ok)),
+            "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
+            "baseline": m["baseline"],
+            "one_at_a_time_fp64_gpu": {"matches_per_s": base, "seconds_per_stream": m["fp64_seconds"]},
+            "one_at_a_time_this_engine": {"matches_per_s": alone, "seconds_per_stream": m["engine_alone_seconds"]},
+            "speedup_vs_one_at_a_time_fp64": m["thr"] / base if base else None,
+            "speedup_vs_one_at_a_time_this_engine": m["thr"] / alone if alone else None,
+            "per_request": m["per_request"], "fit": m["fit"], "prep_seconds": m["prep_seconds"],
+            "clocks": m["clocks"]}
+
+
+def run_serving(args):
+    import logging
+    logging.disable(logging.INFO)
+    iters = args.iters or 50
+    sig_err = args.sigma_error if args.sigma_error is not None else 0.01
+    R = args.requests
+    lanes = () if args.lanes in ("", "none") else tuple(int(b) for b in args.lanes.split(","))
+    ekw = {"max_active": args.max_active, "lanes": lanes, "line_search_precision": args.line_search}
+    baseline = args.baseline if not args.no_fp64 else "none"
+    m = serving_measure(R, args.seed, iters, sig_err, ekw, baseline)
+    summ = serving_summary(m, R, iters, sig_err, ekw)
+    ok, stream = m["ok"], m["stream"]
     # CPU: the FP64 C/OpenMP oracle's per-call timings on the median request x its served call counts
     cpu = None
     if not args.no_cpu_baseline:
-        mid = stream[int(order[R // 2])]
+        mid = stream[int(np.argsort(m["sizes"])[R // 2])]
         served = next((r for r in ok if r.rid == mid.rid), None)
         if served is not None:
             c = served.result["calls"]
@@ -851,26 +957,12 @@ def run_serving(args):
             cpu["sample"] = "median request (V=%d): " % mid.n + cpu["sample"]
     h2d = int(sum(r.v0.nbytes + r.v1.nbytes + r.f0.nbytes + r.f1.nbytes for r in ok))
     d2h = int(sum(r.result["at"].numel() * 8 for r in ok))
-    _line(args, "served surface matches/s", thr, "matches/s", True, config,
-          {"ms_per_step": 1e3 * span / max(1, len(ok)), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
-           "p99_ms": 1e3 * float(np.percentile(lat, 99)), "capacity_closed_loop": cap,
-           "offered_rate": 0.8 * cap, "span_s": span, "failed": st["failed"], "rounds": st["rounds"],
-           "mean_batch": st["mean_batch"], "max_batch": st["max_batch"], "max_active": st["max_active"],
-           "lane_rounds": st["lane_rounds"],
-           "iterations_mean": float(its.mean()), "iterations_min": int(its.min()),
-           "value_refinements": int(sum(r.result["calls"].get("refine", 0) for r in ok)),
-           "values": int(sum(r.result["calls"]["value"] for r in ok)),
-           "converged": int(sum(r.result["converged"] for r in ok)),
-           "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
-           "one_at_a_time_fp64_gpu": {"matches_per_s": base_thr, "seconds_per_stream": pred,
-                                      "per_iter_fit_s": coef_it, "setup_fit_s": coef_set},
-           "one_at_a_time_fp32c_engine": {"matches_per_s": R / pred32 if pred32 else None,
-                                          "seconds_per_stream": pred32,
-                                          "per_iter_fit_s": coef_it32, "setup_fit_s": coef_set32},
-           "samples": samples, "speedup_vs_one_at_a_time_fp64": thr / base_thr if base_thr else None, "prep_seconds": t_prep, "clocks": clk,
-           "cpu_baseline": cpu,
-           "e2e": {"value": thr, "unit": "matches/s", "h2d_bytes_per_step": h2d // max(1, len(ok)),
-                   "d2h_bytes_per_step": d2h // max(1, len(ok))}})
+    config = {"workload": summ.pop("workload")}
+    extra = dict(summ)
+    extra.update({"ms_per_step": 1e3 * m["span"] / max(1, len(ok)), "cpu_baseline": cpu,
+                  "e2e": {"value": m["thr"], "unit": "matches/s", "h2d_bytes_per_step": h2d // max(1, len(ok)),
+                          "d2h_bytes_per_step": d2h // max(1, len(ok))}})
+    _line(args, "served surface matches/s", m["thr"], "matches/s", True, config, extra)
     return 0
 
 
@@ -1083,8 +1175,11 @@ def main():
             oracle.set_num_threads(cores)
             rows = cpu_sample_rows(oracle, x, y, a, p, args.cpu_seconds)
             rng = np.random.default_rng(args.seed + 3)
-            idx = np.sort(rng.choice(min(n, 1 << 16), min(rows, 1 << 16), replace=False))
+            idx = np.sort(rng.choice(n, min(rows, n), replace=False))   # rows drawn from all targets
             ref_out, ref_t = cpu_ops(oracle, x[idx], y, a, p[idx])
+            if fp64 is not None:   # the FP64 GPU path on the same rows
+                xi, pi = xd[idx.tolist()].contiguous(), pd[idx.tolist()].contiguous()
+                f64_rows = {o[0]: run_op(o, k64[o[1]], xi, yd, ad, pi).cpu().numpy() for o in OPS}
             cpu_pairs_s = 4.0 * len(idx) * n / sum(ref_t.values())
             cpu = {"value": cpu_pairs_s, "unit": "pairs/s", "cores": cores, "kind": "port",
                    "sample": "%d target rows x %d sources, 4 ops (FP64 C/OpenMP restatement of "
@@ -1099,7 +1194,7 @@ def main():
                                                    np.maximum(np.linalg.norm(ref, axis=1), 1e-300)).max()),
                 }
                 if fp64 is not None:
-                    o64 = f64_out[o[0]][idx.tolist()].cpu().numpy()
+                    o64 = f64_rows[o[0]]
                     acc[o[0]]["fp64_rel_l2_global"] = float(np.linalg.norm(o64 - ref) / np.linalg.norm(ref))
 
         launches = args.steps * sum(LAUNCHES_PER_OP[o[2]] for o in OPS)
@@ -1119,6 +1214,9 @@ def main():
             "gpu_launches": launches, "clocks": clk, "per_op": per_op, "accuracy_vs_fp64_oracle": acc,
             "fp64_gpu_path": fp64,
         }
+        if world == 1 and not args.no_matching:
+            del flush
+            line["surface_matching"], line["served_matching"] = matching_records(args)
         print(json.dumps(line), flush=True)
     workspace.clear()
     if world > 1:
