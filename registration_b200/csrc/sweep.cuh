@@ -20,12 +20,28 @@
 // exact for 1 and 2), so each unordered pair is evaluated once: the per-target
 // partial sums are no longer the per-target sums, their weighted total is.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace lddmm {
 
+// An operator may accumulate some outputs scaled by a power of two (cheaper per
+// pair); Op::out_scale(c) is then the exact factor applied when they are written.
+template <class Op, class = void>
+struct op_has_out_scale : std::false_type {};
+template <class Op>
+struct op_has_out_scale<Op, std::void_t<decltype(Op::out_scale(0))>> : std::true_type {};
+
+// An operator may ask for a minimum number of resident blocks per SM
+// (Op::MIN_BLOCKS), which caps its registers per thread.
+template <class Op, class = void>
+struct op_min_blocks : std::integral_constant<int, 1> {};
+template <class Op>
+struct op_min_blocks<Op, std::void_t<decltype(Op::MIN_BLOCKS)>> : std::integral_constant<int, Op::MIN_BLOCKS> {};
+
 template <class Op, bool SYM = false>
-__global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, const typename Op::Params P,
+__global__ void __launch_bounds__(Op::BLOCK, op_min_blocks<Op>::value) sweep_kernel(const SweepGrid grid, const typename Op::Params P,
                                                            double* __restrict__ part) {
     using Real = typename Op::Real;
     constexpr int BLOCK = Op::BLOCK, R = Op::R, TILE = Op::TILE, NS = Op::NS, NOUT = Op::NOUT;
@@ -121,8 +137,11 @@ __global__ void __launch_bounds__(Op::BLOCK) sweep_kernel(const SweepGrid grid, 
                 double* dst = part + (sg.part + (long long)chunk * sg.n_tgt + t) * NOUT;
 #pragma unroll
                 for (int c = 0; c < NOUT; ++c) {
-                    if constexpr (TPS == 1) dst[c] = acc[q].value(c);
-                    else dst[c] = acc[q].value(c, lane);
+                    double v;
+                    if constexpr (TPS == 1) v = acc[q].value(c);
+                    else v = acc[q].value(c, lane);
+                    if constexpr (op_has_out_scale<Op>::value) v *= Op::out_scale(c);
+                    dst[c] = v;
                 }
             }
         }

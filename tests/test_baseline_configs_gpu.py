@@ -10,7 +10,9 @@
   Gaussian bumps (width 0.3, amplitudes N(0, 0.1^2)), Gaussian deformation
   kernel sigma 0.5, current data term sigma 0.5, T = 10, 50 cg iterations at
   most, at sigmaError 1 and at sigmaError 0.02.  The plain FP64 path must
-  reproduce the oracle's accepted-objective trace to 1e-9 relative.
+  take the oracle's decisions and reproduce its accepted-objective trace to
+  1e-9 relative (or 1e-12 of obj0, the scale of the norms whose difference
+  each objective value is).
 * Surface matching at its size: the subdivision-5 icosphere (10,242 vertices,
   20,480 faces) with 8 bumps, Gaussian deformation kernel sigma 0.2, varifold
   sigma 0.1, T = 10: the objective and its gradient at seeded momenta, and
@@ -113,7 +115,9 @@ def test_curve_matching_fp64_trace_equals_oracle(oracle_lib, sig_err):
     cm, got = _gpu_curve(v, vt, sig_err, "fp64", "fp64")
     logging.disable(logging.NOTSET)
     assert got.shape == want.shape, (len(got), len(want))
-    np.testing.assert_allclose(got, want, rtol=1e-9)
+    # each value is a small difference of norms of size obj0 = Norm0 / sigmaError^2
+    # (1.2e4 at sigmaError 0.02): FP64 rounding lives on that scale
+    np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12 * abs(want[0]))
     assert cm.iter == rcm.iter
 
 
