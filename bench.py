@@ -914,7 +914,8 @@ def serving_summary(m, R, iters, sig_err, ekw):
                         "iterations max, Poisson arrivals at 80%% of measured capacity, %d slots, 150 GB HBM budget, "
                         "size lanes %s, line search %s" % (R, sig_err, iters, ekw.get("max_active", 64), lanes,
                                                           ekw.get("line_search_precision", "auto")),
-            "matches_per_s": m["thr"], "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "matches_per_s": m["cap"], "matches_per_s_at_80pct_load": m["thr"],
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)),
             "p99_ms": 1e3 * float(np.percentile(lat, 99)), "capacity_closed_loop": m["cap"],
             "offered_rate": 0.8 * m["cap"], "span_s": m["span"], "failed": st["failed"], "rounds": st["rounds"],
             "mean_batch": st["mean_batch"], "max_batch": st["max_batch"], "max_active": st["max_active"],
@@ -926,8 +927,12 @@ def serving_summary(m, R, iters, sig_err, ekw):
             "baseline": m["baseline"],
             "one_at_a_time_fp64_gpu": {"matches_per_s": base, "seconds_per_stream": m["fp64_seconds"]},
             "one_at_a_time_this_engine": {"matches_per_s": alone, "seconds_per_stream": m["engine_alone_seconds"]},
-            "speedup_vs_one_at_a_time_fp64": m["thr"] / base if base else None,
-            "speedup_vs_one_at_a_time_this_engine": m["thr"] / alone if alone else None,
+            # sustained throughput = the closed-loop capacity (every request queued at
+            # t = 0, the engine saturated); the 80%-load stream gives the latencies and
+            # its own R / span, which a short stream's tail (its last large arrivals) bounds
+            "speedup_vs_one_at_a_time_fp64": m["cap"] / base if base else None,
+            "speedup_vs_one_at_a_time_this_engine": m["cap"] / alone if alone else None,
+            "speedup_at_80pct_load_vs_one_at_a_time_fp64": m["thr"] / base if base else None,
             "per_request": m["per_request"], "fit": m["fit"], "prep_seconds": m["prep_seconds"],
             "clocks": m["clocks"]}
 

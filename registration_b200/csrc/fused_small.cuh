@@ -1,0 +1,411 @@
+// Single-launch geodesic shooting and Hamiltonian adjoint for small point sets.
+//
+// For n <= kFusedMaxPoints the T Euler steps of landmarkDirectEvolutionEuler
+// (py-lddmm/pointEvolution.py:666-730) and the T backward steps of
+// landmarkHamiltonianCovector (pointEvolution.py:735-765) each run as ONE
+// kernel on one thread-block cluster of C <= 8 CTAs instead of a sweep and a
+// combine launch per step (plus bounding-box and pack launches): at a few
+// hundred points every launch is a few microseconds of mostly idle GPU.
+//
+// Work split: CTA r of the cluster owns the targets [r*nc, (r+1)*nc), nc =
+// ceil(n / C) <= 128.  Its 256 threads are tpt target slots (tpt = the next
+// power of two >= nc) times S = 256 / tpt source groups; group g sums the
+// sources [g*n/S, (g+1)*n/S) of its target (FP32 partials over 32 sources
+// folded into TwoSum pairs, or plain FP64), and the S group sums of a target
+// are added in group order in FP64.  Every result is a function of the shape
+// and the data only (no atomics), so repeated calls are bit-identical.
+//
+// Step t: every CTA packs all n source records (position in the packing
+// frame, weights) from the step's FP64 state into its shared memory, sums,
+// and the slot-0 thread of each target applies the FP64 update and stores the
+// next state row in global memory.  A cluster barrier (arrive.release /
+// wait.acquire) then makes those rows visible to the other CTAs of the
+// cluster, which read them with ld.global.cg (L2, no stale L1 lines) when they
+// pack the next step.  The packing frame is the centre of the bounding box of
+// the initial points (min / max exact in FP64, computed by every CTA over all
+// points, so every CTA uses the same centre).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <set>
+#include <utility>
+
+#include "host.h"
+#include "kfun.cuh"
+#include "sweep.cuh"
+#include "sweep_dispatch.cuh"
+
+namespace lddmm {
+
+constexpr int kFusedThreads = 256;
+constexpr long long kFusedMaxPoints = 1024;
+constexpr int kFusedMaxCluster = 8;
+constexpr int kFusedTargetsPerCta = 128;
+
+struct FusedShape {
+    int C;    // CTAs in the cluster
+    int nc;   // targets per CTA
+    int tpt;  // target slots per CTA (power of two >= nc)
+    int S;    // source groups
+};
+
+inline FusedShape fused_shape(long long n) {
+    FusedShape f;
+    f.C = (int)std::max(1LL, std::min<long long>(kFusedMaxCluster, (n + kFusedTargetsPerCta - 1) / kFusedTargetsPerCta));
+    f.nc = (int)((n + f.C - 1) / f.C);
+    f.tpt = 1;
+    while (f.tpt < f.nc) f.tpt <<= 1;
+    f.S = kFusedThreads / f.tpt;
+    return f;
+}
+
+LDDMM_D unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+LDDMM_D unsigned cluster_size() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+// All threads of every CTA of the cluster: prior memory operations (global and
+// shared) are visible to the cluster after the wait.
+LDDMM_D void cluster_sync_acq_rel() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// FP64 loads of state written by other CTAs of the cluster in this launch: L2 only.
+LDDMM_D double ldcg(const double* p) { return __ldcg(p); }
+
+// Centre of the bounding box of x[0..n) (d coordinates) into c[0..3); block-wide,
+// `scratch` holds 2 * 3 * kFusedThreads doubles.
+LDDMM_D void fused_bbox_center(const double* x, long long n, int d, double* scratch, double* c) {
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool any = false;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int j = 0; j < d; ++j) {
+            const double v = x[i * d + j];
+            lo[j] = any ? fmin(lo[j], v) : v;
+            hi[j] = any ? fmax(hi[j], v) : v;
+        }
+        any = true;
+    }
+    for (int j = 0; j < 3; ++j) {
+        scratch[(2 * j) * kFusedThreads + threadIdx.x] = any ? lo[j] : INFINITY;
+        scratch[(2 * j + 1) * kFusedThreads + threadIdx.x] = any ? hi[j] : -INFINITY;
+    }
+    __syncthreads();
+    for (int s = kFusedThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            for (int j = 0; j < 3; ++j) {
+                double* L = scratch + (2 * j) * kFusedThreads;
+                double* H = scratch + (2 * j + 1) * kFusedThreads;
+                L[threadIdx.x] = fmin(L[threadIdx.x], L[threadIdx.x + s]);
+                H[threadIdx.x] = fmax(H[threadIdx.x], H[threadIdx.x + s]);
+            }
+        }
+        __syncthreads();
+    }
+    for (int j = 0; j < 3; ++j)
+        c[j] = j < d ? 0.5 * (scratch[(2 * j) * kFusedThreads] + scratch[(2 * j + 1) * kFusedThreads]) : 0.0;
+    __syncthreads();
+}
+
+// FP64 block sum with a fixed tree (thread 0 gets the total); scratch >= kFusedThreads doubles.
+LDDMM_D double fused_block_sum(double v, double* scratch) {
+    scratch[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kFusedThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) scratch[threadIdx.x] += scratch[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+template <class Real>
+struct FusedRec;  // one packed record: position and up to 8 values
+template <>
+struct FusedRec<float> {
+    float4 p, v0, v1;
+};
+template <>
+struct FusedRec<double> {
+    double4a p, v0, v1;
+};
+
+template <class Real>
+LDDMM_D void fused_store(FusedRec<Real>& r, const double* pos, int d, double s, const double* c, const double* v,
+                         int nv) {
+    Real q[4] = {0, 0, 0, 0}, w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < d; ++j) q[j] = (Real)((pos[j] - c[j]) * s);
+    for (int j = 0; j < nv; ++j) w[j] = (Real)v[j];
+    if constexpr (sizeof(Real) == 4) {
+        r.p = make_float4(q[0], q[1], q[2], 0.f);
+        r.v0 = make_float4(w[0], w[1], w[2], w[3]);
+        r.v1 = make_float4(w[4], w[5], w[6], w[7]);
+    } else {
+        r.p = double4a{q[0], q[1], q[2], 0.0};
+        r.v0 = double4a{w[0], w[1], w[2], w[3]};
+        r.v1 = double4a{w[4], w[5], w[6], w[7]};
+    }
+}
+
+template <class Real>
+LDDMM_D void fused_pos(const FusedRec<Real>& r, Real* x) {
+    x[0] = r.p.x;
+    x[1] = r.p.y;
+    x[2] = r.p.z;
+}
+template <class Real>
+LDDMM_D void fused_vals(const FusedRec<Real>& r, Real* v) {
+    v[0] = r.v0.x;
+    v[1] = r.v0.y;
+    v[2] = r.v0.z;
+    v[3] = r.v0.w;
+    v[4] = r.v1.x;
+    v[5] = r.v1.y;
+}
+
+template <class Real, int KIND, int DEG>
+LDDMM_D Real fused_k(const Real* pk, Real r2) {
+    if constexpr (sizeof(Real) == 4) return kval32<KIND, DEG>(pk, r2);
+    else return kval64<KIND, DEG>(pk, r2);
+}
+template <class Real, int KIND, int QDEG>
+LDDMM_D Real fused_kd(const Real* pq, Real r2) {
+    if constexpr (sizeof(Real) == 4) return kdiff32<KIND, QDEG>(pq, r2);
+    else return kdiff64<KIND, QDEG>(pq, r2);
+}
+
+template <class Real, int N>
+using FusedAcc = std::conditional_t<sizeof(Real) == 4, AccF32C<N>, AccF64<N>>;
+
+struct FusedCoef {
+    double pk[5];
+    double pq[4];
+};
+
+// ---- shooting: xt[t+1] = xt[t] + dt K(xt[t]) at[t]; energy = rw dt sum_t <at[t], K at[t]> ----
+template <class Real, int KIND, int DEG, int D>
+__global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double* __restrict__ x0,
+                                                                    const double* __restrict__ at, long long n,
+                                                                    int T, double dt, double scale, FusedCoef cf,
+                                                                    double rw, FusedShape fs, double* xt,
+                                                                    double* energy, double* epart) {
+    extern __shared__ __align__(32) unsigned char fused_smem[];
+    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
+    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * n);
+    double* scratch = red + kFusedThreads * D;
+    const int rank = (int)cluster_rank();
+    const int tid = threadIdx.x;
+    const int local = tid % fs.tpt, g = tid / fs.tpt;
+    const long long k = (long long)rank * fs.nc + local;
+    const bool owner = local < fs.nc && k < n;
+    const long long j0 = g * n / fs.S, j1 = (g + 1) * n / fs.S;
+    Real pk[5];
+    for (int j = 0; j < 5; ++j) pk[j] = (Real)cf.pk[j];
+    double c[3];
+    fused_bbox_center(x0, n, D, scratch, c);
+    const long long N = n * D;
+    if (owner && g == 0)
+        for (int j = 0; j < D; ++j) xt[k * D + j] = x0[k * D + j];
+    double e_acc = 0.0;
+    for (int t = 0; t < T; ++t) {
+        const double* xs = t == 0 ? x0 : xt + (long long)t * N;
+        const double* as = at + (long long)t * N;
+        for (long long i = tid; i < n; i += kFusedThreads) {
+            double p[3], v[3];
+            for (int j = 0; j < D; ++j) {
+                p[j] = t == 0 ? xs[i * D + j] : ldcg(xs + i * D + j);
+                v[j] = as[i * D + j];
+            }
+            fused_store<Real>(rec[i], p, D, scale, c, v, D);
+        }
+        __syncthreads();
+        if (owner) {
+            Real xk[3];
+            fused_pos<Real>(rec[k], xk);
+            FusedAcc<Real, D> acc;
+            acc.zero();
+            constexpr int FOLD = sizeof(Real) == 4 ? 32 : 1 << 30;
+            for (long long jb = j0; jb < j1; jb += FOLD) {
+                acc.begin_fold();
+                const long long je = jb + FOLD < j1 ? jb + FOLD : j1;
+                for (long long j = jb; j < je; ++j) {
+                    Real y[3], w[6];
+                    fused_pos<Real>(rec[j], y);
+                    fused_vals<Real>(rec[j], w);
+                    Real r2 = 0;
+#pragma unroll
+                    for (int q = 0; q < D; ++q) {
+                        const Real dq = xk[q] - y[q];
+                        r2 = q == 0 ? dq * dq : r2 + dq * dq;
+                    }
+                    const Real kv = fused_k<Real, KIND, DEG>(pk, r2);
+#pragma unroll
+                    for (int q = 0; q < D; ++q) acc.fma(q, kv, w[q]);
+                }
+                acc.end_fold();
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) red[(g * fs.tpt + local) * D + q] = acc.value(q);
+        }
+        __syncthreads();
+        if (owner && g == 0) {
+            for (int q = 0; q < D; ++q) {
+                double v = 0.0;
+                for (int gg = 0; gg < fs.S; ++gg) v += red[(gg * fs.tpt + local) * D + q];
+                const double x = t == 0 ? xs[k * D + q] : ldcg(xs + k * D + q);
+                e_acc += as[k * D + q] * v;
+                __stcg(xt + (long long)(t + 1) * N + k * D + q, x + dt * v);
+            }
+        }
+        cluster_sync_acq_rel();
+    }
+    if (energy != nullptr) {
+        const double e = fused_block_sum(e_acc, scratch);
+        if (tid == 0) __stcg(epart + rank, e);
+        cluster_sync_acq_rel();
+        if (rank == 0 && tid == 0) {
+            double s = 0.0;
+            for (int r = 0; r < fs.C; ++r) s += ldcg(epart + r);
+            energy[0] = rw * dt * s;
+        }
+    }
+}
+
+// ---- adjoint: pxt[T] = px1; pxt[t] = pxt[t+1] + dt dscale sum_l F(x_k, x_l) (x'_k - x'_l) <u_k, v_l>,
+//      u = (p - 2 rw a, a), v = (a, p) with p = pxt[t+1], a = at[t]; dat[t] = 2 rw at[t] - pxt[t+1] ----
+template <class Real, int KIND, int QDEG, int D>
+__global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* __restrict__ xt,
+                                                                  const double* __restrict__ at,
+                                                                  const double* __restrict__ px1, long long n, int T,
+                                                                  double dt, double scale, double dscale,
+                                                                  FusedCoef cf, double rw, FusedShape fs, double* pxt,
+                                                                  double* dat) {
+    extern __shared__ __align__(32) unsigned char fused_smem[];
+    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
+    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * n);
+    double* scratch = red + kFusedThreads * D;
+    const int rank = (int)cluster_rank();
+    const int tid = threadIdx.x;
+    const int local = tid % fs.tpt, g = tid / fs.tpt;
+    const long long k = (long long)rank * fs.nc + local;
+    const bool owner = local < fs.nc && k < n;
+    const long long j0 = g * n / fs.S, j1 = (g + 1) * n / fs.S;
+    Real pq[4];
+    for (int j = 0; j < 4; ++j) pq[j] = (Real)cf.pq[j];
+    double c[3];
+    fused_bbox_center(xt, n, D, scratch, c);   // frame of the trajectory's first step
+    const long long N = n * D;
+    if (owner && g == 0)
+        for (int j = 0; j < D; ++j) pxt[(long long)T * N + k * D + j] = px1[k * D + j];
+    for (int t = T - 1; t >= 0; --t) {
+        const double* ps = t == T - 1 ? px1 : pxt + (long long)(t + 1) * N;
+        const double* xs = xt + (long long)t * N;
+        const double* as = at + (long long)t * N;
+        for (long long i = tid; i < n; i += kFusedThreads) {
+            double v[6];
+            for (int j = 0; j < D; ++j) {
+                v[j] = as[i * D + j];
+                v[D + j] = t == T - 1 ? ps[i * D + j] : ldcg(ps + i * D + j);
+            }
+            fused_store<Real>(rec[i], xs + i * D, D, scale, c, v, 2 * D);
+        }
+        __syncthreads();
+        double pk_next[3] = {0, 0, 0}, ak[3] = {0, 0, 0};
+        if (owner) {
+            Real xk[3], u[6];
+            fused_pos<Real>(rec[k], xk);
+            for (int j = 0; j < D; ++j) {
+                ak[j] = as[k * D + j];
+                pk_next[j] = t == T - 1 ? ps[k * D + j] : ldcg(ps + k * D + j);
+                u[j] = (Real)(pk_next[j] - 2.0 * rw * ak[j]);
+                u[D + j] = (Real)ak[j];
+            }
+            FusedAcc<Real, D> acc;
+            acc.zero();
+            constexpr int FOLD = sizeof(Real) == 4 ? 32 : 1 << 30;
+            for (long long jb = j0; jb < j1; jb += FOLD) {
+                acc.begin_fold();
+                const long long je = jb + FOLD < j1 ? jb + FOLD : j1;
+                for (long long j = jb; j < je; ++j) {
+                    Real y[3], w[6], dx[3];
+                    fused_pos<Real>(rec[j], y);
+                    fused_vals<Real>(rec[j], w);
+                    Real r2 = 0, dot = 0;
+#pragma unroll
+                    for (int q = 0; q < D; ++q) {
+                        dx[q] = xk[q] - y[q];
+                        r2 = q == 0 ? dx[q] * dx[q] : r2 + dx[q] * dx[q];
+                    }
+#pragma unroll
+                    for (int q = 0; q < 2 * D; ++q) dot = q == 0 ? u[0] * w[0] : dot + u[q] * w[q];
+                    const Real gv = fused_kd<Real, KIND, QDEG>(pq, r2) * dot;
+#pragma unroll
+                    for (int q = 0; q < D; ++q) acc.fma(q, gv, dx[q]);
+                }
+                acc.end_fold();
+            }
+#pragma unroll
+            for (int q = 0; q < D; ++q) red[(g * fs.tpt + local) * D + q] = acc.value(q);
+        }
+        __syncthreads();
+        if (owner && g == 0) {
+            for (int q = 0; q < D; ++q) {
+                double f = 0.0;
+                for (int gg = 0; gg < fs.S; ++gg) f += red[(gg * fs.tpt + local) * D + q];
+                __stcg(pxt + (long long)t * N + k * D + q, pk_next[q] + dt * (dscale * f));
+                if (dat != nullptr) dat[(long long)t * N + k * D + q] = 2.0 * rw * ak[q] - pk_next[q];
+            }
+        }
+        cluster_sync_acq_rel();
+    }
+}
+
+template <class Real>
+inline size_t fused_dyn_smem(long long n, int D) {
+    return sizeof(FusedRec<Real>) * (size_t)n + sizeof(double) * kFusedThreads * (size_t)D +
+           sizeof(double) * 6 * kFusedThreads;
+}
+
+// Launches `kernel` on one cluster of fs.C CTAs.
+template <class Kern, class... Args>
+int launch_fused(Kern kernel, const FusedShape& fs, size_t smem, cudaStream_t st, Args... args) {
+    // the shared-memory opt-in, once per (device, kernel)
+    static std::mutex mu;
+    static std::set<std::pair<int, const void*>> done;
+    int dev = 0;
+    LDDMM_TRY(cuda_check(cudaGetDevice(&dev), "fused: cudaGetDevice"));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
+        if (done.count(key) == 0) {
+            LDDMM_TRY(cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)(sizeof(FusedRec<double>) * kFusedMaxPoints +
+                                                            sizeof(double) * kFusedThreads * 9)),
+                                 "fused kernel attribute"));
+            done.insert(key);
+        }
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(fs.C, 1, 1);
+    cfg.blockDim = dim3(kFusedThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = fs.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cuda_check(cudaLaunchKernelEx(&cfg, kernel, args...), "fused launch");
+}
+
+}  // namespace lddmm

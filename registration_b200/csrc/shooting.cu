@@ -19,6 +19,7 @@
 // adjoint) update in FP64, writes the packed planes of the next step and the
 // step's energy partials (one per combine block; the grid size depends only on
 // n, so the reduction order is fixed).
+#include "fused_small.cuh"
 #include "host.h"
 #include "ops2.cuh"
 #include "pack.cuh"
@@ -224,11 +225,27 @@ int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     return cuda_check(cudaGetLastError(), "shoot");
 }
 
+// n <= kFusedMaxPoints (and d >= 2): all T steps in one cluster launch (fused_small.cuh)
+template <class Real, int KIND, int DEG, int D>
+int shoot_fused(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
+    const FusedShape fs = fused_shape(a.n);
+    double* epart = ws.take<double>(kFusedMaxCluster);
+    if (ws.measuring()) return LDDMM_OK;
+    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
+    FusedCoef cf{};
+    for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
+    for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
+    const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
+    return launch_fused(shoot_fused_kernel<Real, KIND, DEG, D>, fs, fused_dyn_smem<Real>(a.n, D), st, a.x0, a.at,
+                        (long long)a.n, a.T, dt, ks.scale, cf, a.rw, fs, a.xt, a.energy, epart);
+}
+
 template <class Real>
 int shoot_run(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     return dispatch_kind_p(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(deg)::value, D_ = decltype(D)::value;
+            if (a.n <= kFusedMaxPoints && a.d == D_) return shoot_fused<Real, K_, P_, D_>(a, ws, st);
             if (a.n <= kSmallTargets) return shoot_impl<Real, K_, P_, D_, true>(a, ws, st);
             return shoot_impl<Real, K_, P_, D_>(a, ws, st);
         });
@@ -360,11 +377,25 @@ int cov_impl(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     return cuda_check(cudaGetLastError(), "covector");
 }
 
+template <class Real, int KIND, int QDEG, int D>
+int cov_fused(const CovArgs& a, Workspace& ws, cudaStream_t st) {
+    const FusedShape fs = fused_shape(a.n);
+    if (ws.measuring()) return LDDMM_OK;
+    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
+    FusedCoef cf{};
+    for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
+    for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
+    const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
+    return launch_fused(cov_fused_kernel<Real, KIND, QDEG, D>, fs, fused_dyn_smem<Real>(a.n, D), st, a.xt, a.at,
+                        a.px1, (long long)a.n, a.T, dt, ks.scale, ks.dscale, cf, a.rw, fs, a.pxt, a.dat);
+}
+
 template <class Real>
 int cov_run(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     return dispatch_kind_q(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, Q_ = decltype(deg)::value, D_ = decltype(D)::value;
+            if (a.n <= kFusedMaxPoints && a.d == D_) return cov_fused<Real, K_, Q_, D_>(a, ws, st);
             if (a.n <= kSmallTargets) return cov_impl<Real, K_, Q_, D_, true>(a, ws, st);
             return cov_impl<Real, K_, Q_, D_>(a, ws, st);
         });
