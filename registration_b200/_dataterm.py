@@ -58,11 +58,13 @@ def cell_geometry(vertices, cells):
     return (x[0] + x[1]) / 2, x[1] - x[0]
 
 
-def dataterm(norm, vertices, dshape, tgt_centers, tgt_vectors, K, energy=True, grad=False, eps1=1e-10, eps2=1e-10):
+def dataterm(norm, vertices, dshape, tgt_centers, tgt_vectors, K, energy=True, grad=False, eps1=1e-10, eps2=1e-10,
+             energy_out=None):
     """Returns (energy 0-d tensor or None, px tensor or None), on the device.
 
     vertices: (nv, d) of the deformed shape S1 with topology `dshape`;
-    tgt_centers / tgt_vectors: (nc2, d) of S2 (None for Norm0 of S1)."""
+    tgt_centers / tgt_vectors: (nc2, d) of S2 (None for Norm0 of S1);
+    energy_out: a 0-d FP64 device tensor that receives the energy."""
     require_cuda()
     if K.name == 'none':
         raise ValueError("a kernel is required")
@@ -77,7 +79,10 @@ def dataterm(norm, vertices, dshape, tgt_centers, tgt_vectors, K, energy=True, g
         c2, s2 = to_dev(tgt_centers), to_dev(tgt_vectors)
         nc2 = c2.shape[0]
     sfx = _suffix(K.precision)
-    e = torch.empty((), dtype=torch.float64, device=v.device) if energy else None
+    if energy and energy_out is not None:
+        e = energy_out
+    else:
+        e = torch.empty((), dtype=torch.float64, device=v.device) if energy else None
     px = torch.empty((nv, d), dtype=torch.float64, device=v.device) if grad else None
     wsb = _lib.query("lddmm_dataterm_%s_workspace" % sfx, k, NORMS[norm], nv, d, nc, nc2, int(K.order),
                      1 if energy else 0, 1 if grad else 0)

@@ -106,29 +106,44 @@ class DeviceMatching:
                 getattr(mod, name + 'NormGradient', None))
         return (self.param.fun_obj0, self.param.fun_obj, self.param.fun_objGrad) == want
 
-    def _data_energy(self, vertices, K=None):
-        """fun_obj(fvDef, fv1, KparDist) / sigmaError^2 as a device scalar."""
+    def _data_raw(self, vertices, K=None, out=None):
+        """fun_obj(fvDef, fv1, KparDist) (not yet divided by sigmaError^2) as a
+        device scalar; the fast path writes it into the 0-d tensor `out` if given."""
         K = self._Kval if K is None else K
         if self._fast_data:
             e, _ = _dt.dataterm(self.param.errorType, vertices, self._dshape, self._tc, self._tv,
-                                K, energy=True, grad=False)
-            return e / (self.param.sigmaError ** 2)
+                                K, energy=True, grad=False, energy_out=out)
+            return e
         ff = self.shape_copy(self.fvDef)
         ff.updateVertices(vertices)
-        return torch.tensor(self.param.fun_obj(ff, self.fv1, K) / self.param.sigmaError ** 2,
-                            dtype=torch.float64, device=self.x0.device)
+        e = torch.tensor(self.param.fun_obj(ff, self.fv1, K), dtype=torch.float64, device=self.x0.device)
+        if out is not None:
+            out.copy_(e)
+            return out
+        return e
+
+    def _data_energy(self, vertices, K=None):
+        """fun_obj(fvDef, fv1, KparDist) / sigmaError^2 as a device scalar."""
+        return self._data_raw(vertices, K) / (self.param.sigmaError ** 2)
+
+    def _combine(self, ereg, data_raw):
+        """obj0 + deformation energy + data term / sigmaError^2 from host doubles
+        (one formula for the eager, graphed and refined values)."""
+        return self.obj0 + (ereg + data_raw / self.param.sigmaError ** 2)
 
     def _trial_value(self, e_reg, x_end):
         """obj0 + deformation energy + data term, as compared by the line search."""
-        v = self.obj0 + float(e_reg + self._data_energy(x_end))
+        host = torch.stack([e_reg, self._data_raw(x_end)]).cpu().numpy()
+        ereg = float(host[0])
+        v = self._combine(ereg, float(host[1]))
         if self._auto:
-            v = _Value(v, self, float(e_reg), x_end, value_bound(self, self._noise, self.obj0))
+            v = _Value(v, self, ereg, x_end, value_bound(self, self._noise, self.obj0))
         return v
 
     def exact_value(self, ereg, x_end):
         """The objective with an FP64 data-term value (refinement of a _Value)."""
         self.calls["refine"] = self.calls.get("refine", 0) + 1
-        return self.obj0 + float(ereg + self._data_energy(x_end, self._K64))
+        return self._combine(ereg, float(self._data_raw(x_end, self._K64)))
 
     def dataTerm(self, _fvDef, _fvInit=None):
         return float(self._data_energy(to_dev(_fvDef.vertices)))
@@ -190,8 +205,11 @@ class DeviceMatching:
         """atTry = at - eps dir, its shot and its data-term value, on static buffers."""
         g = self._graph
         torch.sub(g["at"], torch.mul(g["dir"], g["eps"]), out=g["atTry"])
-        xt, e = evol.shoot(self.x0, g["atTry"], self.param.KparDiff, regweight=self.regweight, with_energy=True)
-        return xt, torch.stack([e, self._data_energy(xt[-1])])
+        out = g["out_buf"]   # [deformation energy, raw data term]: written in place by the two kernels
+        xt, _ = evol.shoot(self.x0, g["atTry"], self.param.KparDiff, regweight=self.regweight, with_energy=True,
+                           energy_out=out[0])
+        self._data_raw(xt[-1], out=out[1])
+        return xt, out
 
     def _graph_update_try(self, dir, eps, objRef):
         """updateTry with the shot and the data-term value replayed from a CUDA
@@ -203,7 +221,8 @@ class DeviceMatching:
         if g is None:
             g = self._graph = {"at": self.at.clone(), "dir": dir.diff.clone(),
                                "eps": torch.full((), float(eps), dtype=torch.float64, device=self.x0.device),
-                               "atTry": torch.empty_like(self.at), "at_src": self.at, "dir_src": dir.diff}
+                               "atTry": torch.empty_like(self.at), "at_src": self.at, "dir_src": dir.diff,
+                               "out_buf": torch.empty(2, dtype=torch.float64, device=self.x0.device)}
             # capture on a side stream with the low-level calls (the torch.cuda.graph
             # context manager also collects garbage and empties the allocator cache)
             side = torch.cuda.Stream()
@@ -229,8 +248,8 @@ class DeviceMatching:
         g["eps"].fill_(float(eps))
         g["graph"].replay()
         host = g["out"].cpu().numpy()
-        ereg, data = float(host[0]), float(host[1])
-        objTry = self.obj0 + (ereg + data)
+        ereg = float(host[0])
+        objTry = self._combine(ereg, float(host[1]))
         if self._auto:
             objTry = _Value(objTry, self, ereg, g["xt"][-1].clone(), value_bound(self, self._noise, self.obj0))
         if np.isnan(objTry):

@@ -20,6 +20,7 @@
 // set 2 (target shape), both weighted per source.  No F x F array is formed.
 #include <type_traits>
 
+#include "dataterm_fused.cuh"
 #include "dataterm_ops.cuh"
 #include "host.h"
 #include "pack.cuh"
@@ -161,12 +162,29 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     return cuda_check(cudaGetLastError(), "dataterm");
 }
 
+// Values alone of at most kFusedMaxCells cells: one cluster launch (dataterm_fused.cuh).
+template <class Real, int KIND, int PDEG, int D>
+int dt_value_fused(const DataArgs& a, Workspace& ws, cudaStream_t st) {
+    const FusedShape fs = fused_shape(a.nc);
+    double* epart = ws.take<double>(kFusedMaxCluster);
+    if (ws.measuring()) return LDDMM_OK;
+    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
+    FusedCoef cf{};
+    for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
+    for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
+    return launch_fused(dt_value_fused_kernel<Real, KIND, PDEG, D>, fs, dt_fused_smem<Real>(), dt_fused_smem<Real>(),
+                        st, a.ncorner, a.norm, a.v, (long long)a.nv, a.cells, (long long)a.nc, a.c2, a.s2,
+                        (long long)a.nc2, a.eps1, a.eps2, ks.scale, cf, fs, epart, a.energy);
+}
+
 template <class Real>
 int dt_run(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     auto go = [&](auto kind, auto pdeg, auto qdeg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(pdeg)::value, Q_ = decltype(qdeg)::value,
                           D_ = decltype(D)::value;
+            if (a.px == nullptr && a.energy != nullptr && a.nc <= kFusedMaxCells && a.d == D_)
+                return dt_value_fused<Real, K_, P_, D_>(a, ws, st);
             if (a.nc <= kSmallTargets) return dt_impl<Real, K_, P_, Q_, D_, true>(a, ws, st);
             return dt_impl<Real, K_, P_, Q_, D_>(a, ws, st);
         });

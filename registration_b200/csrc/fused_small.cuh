@@ -7,23 +7,23 @@
 // combine launch per step (plus bounding-box and pack launches): at a few
 // hundred points every launch is a few microseconds of mostly idle GPU.
 //
-// Work split: CTA r of the cluster owns the targets [r*nc, (r+1)*nc), nc =
-// ceil(n / C) <= 128.  Its 256 threads are tpt target slots (tpt = the next
+// Work split: C = min(8, ceil(n / 32)) CTAs; CTA r of the cluster owns the
+// targets [r*nc, (r+1)*nc), nc = ceil(n / C) <= 128.  Its 256 threads are tpt target slots (tpt = the next
 // power of two >= nc) times S = 256 / tpt source groups; group g sums the
 // sources [g*n/S, (g+1)*n/S) of its target (FP32 partials over 32 sources
 // folded into TwoSum pairs, or plain FP64), and the S group sums of a target
 // are added in group order in FP64.  Every result is a function of the shape
 // and the data only (no atomics), so repeated calls are bit-identical.
 //
-// Step t: every CTA packs all n source records (position in the packing
-// frame, weights) from the step's FP64 state into its shared memory, sums,
-// and the slot-0 thread of each target applies the FP64 update and stores the
-// next state row in global memory.  A cluster barrier (arrive.release /
-// wait.acquire) then makes those rows visible to the other CTAs of the
-// cluster, which read them with ld.global.cg (L2, no stale L1 lines) when they
-// pack the next step.  The packing frame is the centre of the bounding box of
-// the initial points (min / max exact in FP64, computed by every CTA over all
-// points, so every CTA uses the same centre).
+// Step t: every CTA sums over the n source records (position in the packing
+// frame, weights) of the step held in its shared memory; the slot-0 thread of
+// each target applies the FP64 update, stores the next state row in global
+// memory (the output) and writes the target's next-step record into the
+// shared memory of every CTA of the cluster (distributed shared memory,
+// double-buffered).  A cluster barrier (arrive.release / wait.acquire) per
+// step orders those writes.  The packing frame is the centre of the bounding
+// box of the initial points (min / max exact in FP64, computed by every CTA
+// over all points, so every CTA uses the same centre).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -38,10 +38,19 @@
 
 namespace lddmm {
 
-constexpr int kFusedThreads = 256;
+#ifndef LDDMM_FUSED_THREADS
+#define LDDMM_FUSED_THREADS 256
+#endif
+#ifndef LDDMM_FUSED_UNROLL
+#define LDDMM_FUSED_UNROLL 1
+#endif
+constexpr int kFusedThreads = LDDMM_FUSED_THREADS;
+constexpr int kFusedUnroll = LDDMM_FUSED_UNROLL;   // inner source loop
 constexpr long long kFusedMaxPoints = 1024;
 constexpr int kFusedMaxCluster = 8;
-constexpr int kFusedTargetsPerCta = 128;
+// targets per CTA before the cluster grows: every CTA of a full cluster then
+// owns <= 128 targets, each target spread over >= 2 source groups
+constexpr int kFusedTargetsPerCta = 32;
 
 struct FusedShape {
     int C;    // CTAs in the cluster
@@ -190,7 +199,31 @@ struct FusedCoef {
     double pq[4];
 };
 
+// The record `r` into the same slot `slot` of every CTA's shared memory
+// (distributed shared memory of the cluster), 16 bytes at a time.
+template <class Real>
+LDDMM_D void fused_broadcast(const FusedRec<Real>& r, FusedRec<Real>* slot, int C) {
+    constexpr int W = sizeof(FusedRec<Real>) / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(&r);
+    const unsigned laddr = (unsigned)__cvta_generic_to_shared(slot);
+    for (int q = 0; q < C; ++q) {
+        unsigned raddr;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(raddr) : "r"(laddr), "r"(q));
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const uint4 v = src[w];
+            asm volatile("st.shared::cluster.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(raddr + 16 * w), "r"(v.x),
+                         "r"(v.y), "r"(v.z), "r"(v.w)
+                         : "memory");
+        }
+    }
+}
+
 // ---- shooting: xt[t+1] = xt[t] + dt K(xt[t]) at[t]; energy = rw dt sum_t <at[t], K at[t]> ----
+// Source records are double-buffered: step t reads buffer t & 1, and the owner
+// of each target writes its step-(t+1) record into buffer (t+1) & 1 of every
+// CTA; the cluster barrier at the end of step t orders those writes before the
+// reads of step t+1 and after every read of step t-1.
 template <class Real, int KIND, int DEG, int D>
 __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double* __restrict__ x0,
                                                                     const double* __restrict__ at, long long n,
@@ -198,8 +231,9 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
                                                                     double rw, FusedShape fs, double* xt,
                                                                     double* energy, double* epart) {
     extern __shared__ __align__(32) unsigned char fused_smem[];
-    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
-    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * n);
+    FusedRec<Real>* rec0 = reinterpret_cast<FusedRec<Real>*>(fused_smem);
+    FusedRec<Real>* rec1 = rec0 + n;
+    double* red = reinterpret_cast<double*>(fused_smem + 2 * sizeof(FusedRec<Real>) * n);
     double* scratch = red + kFusedThreads * D;
     const int rank = (int)cluster_rank();
     const int tid = threadIdx.x;
@@ -212,21 +246,27 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
     double c[3];
     fused_bbox_center(x0, n, D, scratch, c);
     const long long N = n * D;
+    for (long long i = tid; i < n; i += kFusedThreads) fused_store<Real>(rec0[i], x0 + i * D, D, scale, c, at + i * D, D);
+    double xk64[3] = {0, 0, 0};
     if (owner && g == 0)
-        for (int j = 0; j < D; ++j) xt[k * D + j] = x0[k * D + j];
+        for (int j = 0; j < D; ++j) xk64[j] = x0[k * D + j];
+    // every CTA's buffer 0 is complete before any CTA's owners overwrite its buffer 1
+    cluster_sync_acq_rel();
     double e_acc = 0.0;
     for (int t = 0; t < T; ++t) {
-        const double* xs = t == 0 ? x0 : xt + (long long)t * N;
+        const FusedRec<Real>* rec = (t & 1) ? rec1 : rec0;
+        FusedRec<Real>* nxt = (t & 1) ? rec0 : rec1;
         const double* as = at + (long long)t * N;
-        for (long long i = tid; i < n; i += kFusedThreads) {
-            double p[3], v[3];
+        // slot 0: store the row x_t of the output (off the critical path: the next cluster
+        // barrier's release is a step away) and prefetch the momenta the update needs
+        double a_now[3] = {0, 0, 0}, a_next[3] = {0, 0, 0};
+        if (owner && g == 0) {
             for (int j = 0; j < D; ++j) {
-                p[j] = t == 0 ? xs[i * D + j] : ldcg(xs + i * D + j);
-                v[j] = as[i * D + j];
+                xt[(long long)t * N + k * D + j] = xk64[j];
+                a_now[j] = as[k * D + j];
+                if (t + 1 < T) a_next[j] = as[N + k * D + j];
             }
-            fused_store<Real>(rec[i], p, D, scale, c, v, D);
         }
-        __syncthreads();
         if (owner) {
             Real xk[3];
             fused_pos<Real>(rec[k], xk);
@@ -236,6 +276,7 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
             for (long long jb = j0; jb < j1; jb += FOLD) {
                 acc.begin_fold();
                 const long long je = jb + FOLD < j1 ? jb + FOLD : j1;
+#pragma unroll kFusedUnroll
                 for (long long j = jb; j < je; ++j) {
                     Real y[3], w[6];
                     fused_pos<Real>(rec[j], y);
@@ -260,20 +301,26 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
             for (int q = 0; q < D; ++q) {
                 double v = 0.0;
                 for (int gg = 0; gg < fs.S; ++gg) v += red[(gg * fs.tpt + local) * D + q];
-                const double x = t == 0 ? xs[k * D + q] : ldcg(xs + k * D + q);
-                e_acc += as[k * D + q] * v;
-                __stcg(xt + (long long)(t + 1) * N + k * D + q, x + dt * v);
+                e_acc += a_now[q] * v;
+                xk64[q] = xk64[q] + dt * v;
+            }
+            if (t + 1 < T) {
+                FusedRec<Real> r;
+                fused_store<Real>(r, xk64, D, scale, c, a_next, D);
+                fused_broadcast<Real>(r, nxt + k, fs.C);
             }
         }
         cluster_sync_acq_rel();
     }
+    if (owner && g == 0)
+        for (int j = 0; j < D; ++j) xt[(long long)T * N + k * D + j] = xk64[j];
     if (energy != nullptr) {
         const double e = fused_block_sum(e_acc, scratch);
         if (tid == 0) __stcg(epart + rank, e);
         cluster_sync_acq_rel();
         if (rank == 0 && tid == 0) {
             double s = 0.0;
-            for (int r = 0; r < fs.C; ++r) s += ldcg(epart + r);
+            for (int r = 0; r < fs.C; ++r) s += __ldcg(epart + r);
             energy[0] = rw * dt * s;
         }
     }
@@ -281,6 +328,7 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
 
 // ---- adjoint: pxt[T] = px1; pxt[t] = pxt[t+1] + dt dscale sum_l F(x_k, x_l) (x'_k - x'_l) <u_k, v_l>,
 //      u = (p - 2 rw a, a), v = (a, p) with p = pxt[t+1], a = at[t]; dat[t] = 2 rw at[t] - pxt[t+1] ----
+// Records of step t: position x_t, values (a_t, p_{t+1}); double-buffered as in the shot.
 template <class Real, int KIND, int QDEG, int D>
 __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* __restrict__ xt,
                                                                   const double* __restrict__ at,
@@ -289,8 +337,9 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
                                                                   FusedCoef cf, double rw, FusedShape fs, double* pxt,
                                                                   double* dat) {
     extern __shared__ __align__(32) unsigned char fused_smem[];
-    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
-    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * n);
+    FusedRec<Real>* rec0 = reinterpret_cast<FusedRec<Real>*>(fused_smem);
+    FusedRec<Real>* rec1 = rec0 + n;
+    double* red = reinterpret_cast<double*>(fused_smem + 2 * sizeof(FusedRec<Real>) * n);
     double* scratch = red + kFusedThreads * D;
     const int rank = (int)cluster_rank();
     const int tid = threadIdx.x;
@@ -303,30 +352,54 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
     double c[3];
     fused_bbox_center(xt, n, D, scratch, c);   // frame of the trajectory's first step
     const long long N = n * D;
-    if (owner && g == 0)
-        for (int j = 0; j < D; ++j) pxt[(long long)T * N + k * D + j] = px1[k * D + j];
-    for (int t = T - 1; t >= 0; --t) {
-        const double* ps = t == T - 1 ? px1 : pxt + (long long)(t + 1) * N;
-        const double* xs = xt + (long long)t * N;
-        const double* as = at + (long long)t * N;
+    {
+        const double* xs = xt + (long long)(T - 1) * N;
+        const double* as = at + (long long)(T - 1) * N;
         for (long long i = tid; i < n; i += kFusedThreads) {
             double v[6];
             for (int j = 0; j < D; ++j) {
                 v[j] = as[i * D + j];
-                v[D + j] = t == T - 1 ? ps[i * D + j] : ldcg(ps + i * D + j);
+                v[D + j] = px1[i * D + j];
             }
-            fused_store<Real>(rec[i], xs + i * D, D, scale, c, v, 2 * D);
+            fused_store<Real>(rec0[i], xs + i * D, D, scale, c, v, 2 * D);
         }
-        __syncthreads();
-        double pk_next[3] = {0, 0, 0}, ak[3] = {0, 0, 0};
+    }
+    // p_{t+1} of this CTA's targets in FP64, shared by their source groups
+    double* pown = scratch;   // fs.tpt * 3 doubles (the bounding-box scratch is free again)
+    double pn[3] = {0, 0, 0};   // slot 0: the target's p_{t+1}
+    if (owner && g == 0)
+        for (int j = 0; j < D; ++j) {
+            pn[j] = px1[k * D + j];
+            pxt[(long long)T * N + k * D + j] = pn[j];
+            pown[local * 3 + j] = pn[j];
+        }
+    cluster_sync_acq_rel();
+    // slot 0 stores step t's rows of pxt and dat at the start of step t - 1 (off the
+    // critical path: the release of the next cluster barrier is a step away)
+    int pend = -1;
+    double pend_p[3] = {0, 0, 0}, pend_d[3] = {0, 0, 0};
+    auto flush = [&]() {
+        if (pend >= 0)
+            for (int q = 0; q < D; ++q) {
+                pxt[(long long)pend * N + k * D + q] = pend_p[q];
+                if (dat != nullptr) dat[(long long)pend * N + k * D + q] = pend_d[q];
+            }
+        pend = -1;
+    };
+    int b = 0;
+    for (int t = T - 1; t >= 0; --t, b ^= 1) {
+        const FusedRec<Real>* rec = b ? rec1 : rec0;
+        FusedRec<Real>* nxt = b ? rec0 : rec1;
+        const double* as = at + (long long)t * N;
+        if (owner && g == 0) flush();
         if (owner) {
             Real xk[3], u[6];
             fused_pos<Real>(rec[k], xk);
+            // u_k = (p - 2 rw a, a) in FP64, then rounded
             for (int j = 0; j < D; ++j) {
-                ak[j] = as[k * D + j];
-                pk_next[j] = t == T - 1 ? ps[k * D + j] : ldcg(ps + k * D + j);
-                u[j] = (Real)(pk_next[j] - 2.0 * rw * ak[j]);
-                u[D + j] = (Real)ak[j];
+                const double aj = as[k * D + j];
+                u[j] = (Real)(pown[local * 3 + j] - 2.0 * rw * aj);
+                u[D + j] = (Real)aj;
             }
             FusedAcc<Real, D> acc;
             acc.zero();
@@ -334,6 +407,7 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
             for (long long jb = j0; jb < j1; jb += FOLD) {
                 acc.begin_fold();
                 const long long je = jb + FOLD < j1 ? jb + FOLD : j1;
+#pragma unroll kFusedUnroll
                 for (long long j = jb; j < je; ++j) {
                     Real y[3], w[6], dx[3];
                     fused_pos<Real>(rec[j], y);
@@ -357,26 +431,45 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
         }
         __syncthreads();
         if (owner && g == 0) {
+            double pc[3];
             for (int q = 0; q < D; ++q) {
                 double f = 0.0;
                 for (int gg = 0; gg < fs.S; ++gg) f += red[(gg * fs.tpt + local) * D + q];
-                __stcg(pxt + (long long)t * N + k * D + q, pk_next[q] + dt * (dscale * f));
-                if (dat != nullptr) dat[(long long)t * N + k * D + q] = 2.0 * rw * ak[q] - pk_next[q];
+                pc[q] = pn[q] + dt * (dscale * f);
             }
+            if (t > 0) {
+                double v[6];
+                for (int j = 0; j < D; ++j) {
+                    v[j] = as[-N + k * D + j];
+                    v[D + j] = pc[j];
+                }
+                FusedRec<Real> r;
+                fused_store<Real>(r, xt + (long long)(t - 1) * N + k * D, D, scale, c, v, 2 * D);
+                fused_broadcast<Real>(r, nxt + k, fs.C);
+            }
+            for (int q = 0; q < D; ++q) {
+                pend_d[q] = 2.0 * rw * as[k * D + q] - pn[q];
+                pend_p[q] = pc[q];
+                pown[local * 3 + q] = pc[q];
+                pn[q] = pc[q];
+            }
+            pend = t;
         }
         cluster_sync_acq_rel();
     }
+    if (owner && g == 0) flush();
 }
 
 template <class Real>
 inline size_t fused_dyn_smem(long long n, int D) {
-    return sizeof(FusedRec<Real>) * (size_t)n + sizeof(double) * kFusedThreads * (size_t)D +
+    return 2 * sizeof(FusedRec<Real>) * (size_t)n + sizeof(double) * kFusedThreads * (size_t)D +
            sizeof(double) * 6 * kFusedThreads;
 }
 
-// Launches `kernel` on one cluster of fs.C CTAs.
+// Launches `kernel` on one cluster of fs.C CTAs with `smem` bytes of dynamic
+// shared memory (`max_smem`: the kernel's opt-in limit, at least smem).
 template <class Kern, class... Args>
-int launch_fused(Kern kernel, const FusedShape& fs, size_t smem, cudaStream_t st, Args... args) {
+int launch_fused(Kern kernel, const FusedShape& fs, size_t smem, size_t max_smem, cudaStream_t st, Args... args) {
     // the shared-memory opt-in, once per (device, kernel)
     static std::mutex mu;
     static std::set<std::pair<int, const void*>> done;
@@ -387,8 +480,7 @@ int launch_fused(Kern kernel, const FusedShape& fs, size_t smem, cudaStream_t st
         const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
         if (done.count(key) == 0) {
             LDDMM_TRY(cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      (int)(sizeof(FusedRec<double>) * kFusedMaxPoints +
-                                                            sizeof(double) * kFusedThreads * 9)),
+                                                      (int)max_smem),
                                  "fused kernel attribute"));
             done.insert(key);
         }

@@ -236,7 +236,8 @@ int shoot_fused(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
     for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
     const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
-    return launch_fused(shoot_fused_kernel<Real, KIND, DEG, D>, fs, fused_dyn_smem<Real>(a.n, D), st, a.x0, a.at,
+    return launch_fused(shoot_fused_kernel<Real, KIND, DEG, D>, fs, fused_dyn_smem<Real>(a.n, D),
+                        fused_dyn_smem<Real>(kFusedMaxPoints, 3), st, a.x0, a.at,
                         (long long)a.n, a.T, dt, ks.scale, cf, a.rw, fs, a.xt, a.energy, epart);
 }
 
@@ -386,7 +387,8 @@ int cov_fused(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
     for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
     const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
-    return launch_fused(cov_fused_kernel<Real, KIND, QDEG, D>, fs, fused_dyn_smem<Real>(a.n, D), st, a.xt, a.at,
+    return launch_fused(cov_fused_kernel<Real, KIND, QDEG, D>, fs, fused_dyn_smem<Real>(a.n, D),
+                        fused_dyn_smem<Real>(kFusedMaxPoints, 3), st, a.xt, a.at,
                         a.px1, (long long)a.n, a.T, dt, ks.scale, ks.dscale, cf, a.rw, fs, a.pxt, a.dat);
 }
 

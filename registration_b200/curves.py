@@ -47,11 +47,33 @@ class Curve:
 
     def computeCentersLengths(self):
         """edge centres and tangent vectors (curves.py:58-64)"""
-        self.centers, self.lenel = _dt.cell_geometry(self.vertices, self.faces)
+        self._centers, self._lenel = _dt.cell_geometry(self.vertices, self.faces)
+        self._stale = False
 
     def updateVertices(self, x0):
+        """The centres and tangents follow on first use."""
         self.vertices = _copy(x0)
-        self.computeCentersLengths()
+        self._stale = True
+
+    @property
+    def centers(self):
+        if getattr(self, "_stale", False):
+            self.computeCentersLengths()
+        return self._centers
+
+    @centers.setter
+    def centers(self, c):
+        self._centers = c
+
+    @property
+    def lenel(self):
+        if getattr(self, "_stale", False):
+            self.computeCentersLengths()
+        return self._lenel
+
+    @lenel.setter
+    def lenel(self, v):
+        self._lenel = v
 
     def device_shape(self):
         if self._dshape is None:

@@ -37,9 +37,10 @@ def _kernel_args(K):
     return float(K.sigma), int(K.order), _suffix(K.precision)
 
 
-def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False, dt=None):
+def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False, dt=None, energy_out=None):
     """Device call: returns (xt, energy) with energy = sum_t rw dt <a_t, K(x_t) a_t> (a 0-d tensor) or None.
-    dt defaults to 1/T; pass it to shoot a segment of a longer trajectory."""
+    dt defaults to 1/T; pass it to shoot a segment of a longer trajectory.  energy_out: a 0-d FP64
+    device tensor (e.g. a view into a larger buffer) that receives the energy."""
     require_cuda()
     x0d = to_dev(x0)
     atd = to_dev(at)
@@ -48,7 +49,10 @@ def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False, dt=None):
         raise ValueError("x0 must be (N, dim) and at (T, N, dim)")
     sigma, order, sfx = _kernel_args(KparDiff)
     xt = torch.empty((T + 1, n, d), dtype=torch.float64, device=x0d.device)
-    energy = torch.empty((), dtype=torch.float64, device=x0d.device) if with_energy else None
+    if energy_out is not None:
+        energy = energy_out
+    else:
+        energy = torch.empty((), dtype=torch.float64, device=x0d.device) if with_energy else None
     wsb = _lib.query("lddmm_shoot_%s_workspace" % sfx, n, d, T)
     ws = workspace.get(wsb)
     _lib.call("lddmm_shoot_" + sfx, ptr(x0d), n, d, ptr(atd), T, float(dt or 0.0), sigma, order, float(regweight), ptr(xt),

@@ -62,12 +62,34 @@ class Surface:
 
     def computeCentersAreas(self):
         """face centres and area-weighted normals (surfaces.py:61-66)"""
-        self.centers, self.surfel = _dt.cell_geometry(self.vertices, self.faces)
+        self._centers, self._surfel = _dt.cell_geometry(self.vertices, self.faces)
+        self._stale = False
 
     def updateVertices(self, x0):
-        """(surfaces.py:69-75)"""
+        """(surfaces.py:69-75); the centres and normals follow on first use."""
         self.vertices = _copy(x0)
-        self.computeCentersAreas()
+        self._stale = True
+
+    # centres / surfel of the current vertices, recomputed after updateVertices when read
+    @property
+    def centers(self):
+        if getattr(self, "_stale", False):
+            self.computeCentersAreas()
+        return self._centers
+
+    @centers.setter
+    def centers(self, c):
+        self._centers = c
+
+    @property
+    def surfel(self):
+        if getattr(self, "_stale", False):
+            self.computeCentersAreas()
+        return self._surfel
+
+    @surfel.setter
+    def surfel(self, s):
+        self._surfel = s
 
     def flipFaces(self):
         """(surfaces.py:261-263)"""

@@ -1,0 +1,70 @@
+"""Single-launch data-term values (shapes of at most 1024 cells: one
+thread-block cluster computes the cell geometry, the packing frame, the sums
+and the energy) against the FP64 oracle, for the three norms on surfaces and
+the two on curves, NormDef and Norm0, on both sides of the 1024-cell limit.
+Tolerance: fp32c 1e-5, fp64 1e-12, of the target's Norm0 (the scale of the
+norms whose difference NormDef is)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32c": 1e-5, "fp64": 1e-12}
+
+
+def _surface(nf_target, seed):
+    from registration_b200 import geometry as geo
+    rng = np.random.default_rng(seed)
+    lvl = 1
+    while 20 * 4 ** lvl < nf_target:
+        lvl += 1
+    v, f = geo.icosphere(lvl)
+    if len(f) > nf_target:
+        v, f = geo.decimate(v, f, nf_target // 2 + 2, rng)
+    vt = geo.bumped_sphere(v, f, 4, 0.3, 0.1, rng)
+    vd = v + 0.02 * rng.standard_normal(v.shape)
+    return v, f, vt, vd
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("err", ["current", "measure", "varifold"])
+@pytest.mark.parametrize("nf", [80, 320, 1020, 1280])
+def test_surface_values_against_oracle(oracle_lib, precision, err, nf):
+    from oracle import lddmm_ref as ref
+    from registration_b200 import kernelFunctions as kf
+    from registration_b200 import surfaces as sf
+    v, f, vt, vd = _surface(nf, nf)
+    K = kf.Kernel(name="gauss", sigma=0.2, precision=precision)
+    KR = ref.Kernel(name="gauss", sigma=0.2)
+    a, b = sf.Surface(FV=[f, vd]), sf.Surface(FV=[f, vt])
+    ra, rb = ref.Surface(FV=[f, vd]), ref.Surface(FV=[f, vt])
+    n0 = getattr(ref, err + "Norm0")(rb, KR)
+    assert abs(getattr(sf, err + "Norm0")(b, K) - n0) <= TOL[precision] * abs(n0)
+    e = getattr(sf, err + "NormDef")(a, b, K)
+    assert abs(e - getattr(ref, err + "NormDef")(ra, rb, KR)) <= TOL[precision] * abs(n0)
+    assert e == getattr(sf, err + "NormDef")(a, b, K)   # repeatable
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("err", ["current", "measure"])
+@pytest.mark.parametrize("n,d,kname", [(256, 2, "gauss"), (256, 2, "laplacian"), (1000, 3, "gauss"), (1100, 2, "gauss"),
+                                       (7, 2, "laplacian")])
+def test_curve_values_against_oracle(oracle_lib, precision, err, n, d, kname):
+    from oracle import lddmm_ref as ref
+    from registration_b200 import curves as cv
+    from registration_b200 import geometry as geo
+    from registration_b200 import kernelFunctions as kf
+    rng = np.random.default_rng(n + d)
+    c, _ = geo.ellipse_curve(n, 1.0, 0.6)
+    if d == 3:
+        c = np.concatenate([c, 0.1 * np.sin(np.arange(n))[:, None]], axis=1)
+    ct = c + 0.05 * rng.standard_normal(c.shape)
+    cd = c + 0.02 * rng.standard_normal(c.shape)
+    K = kf.Kernel(name=kname, sigma=0.5, order=3, precision=precision)
+    KR = ref.Kernel(name=kname, sigma=0.5, order=3)
+    a, b = cv.Curve(pointSet=cd), cv.Curve(pointSet=ct)
+    ra, rb = ref.Curve(pointSet=cd), ref.Curve(pointSet=ct)
+    n0 = getattr(ref, "curve_" + err + "Norm0")(rb, KR)
+    assert abs(getattr(cv, err + "Norm0")(b, K) - n0) <= TOL[precision] * abs(n0)
+    e_ref = getattr(ref, "curve_" + err + "NormDef")(ra, rb, KR)
+    assert abs(getattr(cv, err + "NormDef")(a, b, K) - e_ref) <= TOL[precision] * abs(n0)
