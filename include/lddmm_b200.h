@@ -267,6 +267,21 @@ LDDMM_API int lddmm_applykdiff11and12_f64(const double* x, int64_t n, int d, con
                                           const double* p, double sigma, int order, double* f, void* workspace,
                                           size_t workspace_bytes, lddmm_stream_t stream);
 
+/* ---- affine kernel parts: KernelSpec(affine = 'affine' | 'euclidean') ----------
+ * No f2py counterpart: py-lddmm/kernelFunctions.py:334-367 (applyK) and
+ * :431-448 (applyDiffKT) add these terms in numpy after the kernel sums.
+ * lddmm_moments_f64: out[i * dimb + j] = sum_l (x_l - c)_i a_l,j  (i < d, j < dimb)
+ *   and out[d * dimb + j] = sum_l a_l,j; x (m, d), a (m, dimb), c (d) or NULL
+ *   for 0; out: d * dimb + dimb doubles; dimb <= 4; FP64, fixed reduction order;
+ *   workspace sized by lddmm_moments_f64_workspace.
+ * lddmm_rows_affine_f64: f[k, j] += sum_q (u[k, q] - c[q]) W[q, j] + b[j]
+ *   u (n, Q), c (Q) or NULL, W (Q, J), b (J) or NULL, f (n, J); Q <= 16, J <= 4. */
+LDDMM_API size_t lddmm_moments_f64_workspace(int64_t m, int d, int dimb);
+LDDMM_API int lddmm_moments_f64(const double* x, int64_t m, int d, const double* a, int dimb, const double* center,
+                                double* out, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_rows_affine_f64(const double* u, int64_t n, int Q, const double* center, const double* W,
+                                    const double* b, int J, double* f, lddmm_stream_t stream);
+
 /* ---- ragged launches: many independent problems in one launch ----------------
  * No single counterpart in the reference (which solves one problem per process);
  * each segment computes exactly what the single-problem entry point above

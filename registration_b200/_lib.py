@@ -29,6 +29,9 @@ SIGNATURES = {
     "lddmm_applykdifft_f64_workspace": (_SZ, [_I64, _I64, _I, _I, _I]),
     "lddmm_applykdifft_f32c": (_I, [_P, _I64, _P, _I64, _P, _P, _I, _I, _I, _D, _I, _P, _P, _SZ, _P]),
     "lddmm_applykdifft_f64": (_I, [_P, _I64, _P, _I64, _P, _P, _I, _I, _I, _D, _I, _P, _P, _SZ, _P]),
+    "lddmm_moments_f64_workspace": (_SZ, [_I64, _I, _I]),
+    "lddmm_moments_f64": (_I, [_P, _I64, _I, _P, _I, _P, _P, _P, _SZ, _P]),
+    "lddmm_rows_affine_f64": (_I, [_P, _I64, _I, _P, _P, _P, _I, _P, _P]),
     "lddmm_applydiv_f32c_workspace": (_SZ, [_I64, _I64, _I]),
     "lddmm_applydiv_f64_workspace": (_SZ, [_I64, _I64, _I]),
     "lddmm_applydiv_f32c": (_I, [_P, _I64, _P, _I64, _P, _I, _D, _I, _P, _P, _SZ, _P]),

@@ -11,7 +11,9 @@ Drop-in rules kept from the reference:
     (kernelFunctions.py:285-298);
   * outputs are fresh float64 arrays: numpy in -> numpy out; CUDA tensors in ->
     CUDA tensors out (stays on the device).
-Only affine='none' is provided (affine kernel parts are outside the hot path).
+Affine kernel parts (``affine='affine'`` or ``'euclidean'``, kernelFunctions.py:
+334-367 and 431-448) are added on the device after the kernel sums, from the
+FP64 moments of the sources (lddmm_moments_f64, lddmm_rows_affine_f64).
 
 Extra keyword: ``precision`` = 'fp32c' (default: FP32 pair arithmetic with
 compensated accumulation, FP64 results) or 'fp64' (plain FP64 on the GPU).
@@ -62,8 +64,21 @@ class KernelSpec:
         else:
             self.name = 'none'
             self.par = []
-        if affine not in ('none', None):
-            raise NotImplementedError("affine kernel components are not part of this library (affine='none' only)")
+        if affine is None:
+            self.affine = 'none'
+        elif affine not in ('none', 'affine', 'euclidean'):
+            raise ValueError("affine must be 'none', 'affine' or 'euclidean'")
+        if self.affine == 'euclidean':
+            # the skew-symmetric basis of the reference (kernelFunctions.py:268-278)
+            s2 = np.sqrt(2.0)
+            if dim == 3:
+                self.affine_basis = [np.array([[0, 1, 0], [-1, 0, 0], [0, 0, 0]]) / s2,
+                                     np.array([[0, 0, 1], [0, 0, 0], [-1, 0, 0]]) / s2,
+                                     np.array([[0, 0, 0], [0, 0, 1], [0, -1, 0]]) / s2]
+            elif dim == 2:
+                self.affine_basis = [np.array([[0, 1], [-1, 0]]) / s2]
+            else:
+                raise ValueError("euclidean kernels are available in dimension 2 or 3 only")
 
 
 class Kernel(KernelSpec):
@@ -97,14 +112,84 @@ class Kernel(KernelSpec):
         if tgt.shape[1] != d:
             raise ValueError("applyK: firstVar and x have different dimensions")
         if self.name == 'none':
-            return output_like(x, torch.zeros((n, dimb), dtype=torch.float64, device=src.device))
-        f = torch.empty((n, dimb), dtype=torch.float64, device=src.device)
-        sfx = _suffix(self.precision)
-        wsb = _lib.query("lddmm_applyk_%s_workspace" % sfx, n, m, d, dimb)
-        ws = workspace.get(wsb)
-        _lib.call("lddmm_applyk_" + sfx, ptr(tgt), n, ptr(src), m, ptr(w), d, dimb, float(self.sigma),
-                  int(self.order), ptr(f), ptr(ws), wsb, stream_handle())
+            f = torch.zeros((n, dimb), dtype=torch.float64, device=src.device)
+        else:
+            f = torch.empty((n, dimb), dtype=torch.float64, device=src.device)
+            sfx = _suffix(self.precision)
+            wsb = _lib.query("lddmm_applyk_%s_workspace" % sfx, n, m, d, dimb)
+            ws = workspace.get(wsb)
+            _lib.call("lddmm_applyk_" + sfx, ptr(tgt), n, ptr(src), m, ptr(w), d, dimb, float(self.sigma),
+                      int(self.order), ptr(f), ptr(ws), wsb, stream_handle())
+        if self.affine != 'none':
+            self._affine_applyk(src, w, tgt, f)
         return output_like(x, f)
+
+    # ---- affine parts (kernelFunctions.py:334-367, 431-448) -------------------
+    def _center_dev(self, d, device):
+        c = np.zeros(d)
+        cc = np.asarray(self.center, dtype=np.float64).reshape(-1)
+        c[:min(d, cc.size)] = cc[:d]
+        return torch.from_numpy(c).to(device)
+
+    def _moments(self, src, w, c):
+        """(M, s) on the host: M = sum_l (x_l - c) w_l^T (d x dimb), s = sum_l w_l (FP64 on the device)."""
+        m, d = src.shape
+        dimb = w.shape[1]
+        out = torch.empty(d * dimb + dimb, dtype=torch.float64, device=src.device)
+        wsb = _lib.query("lddmm_moments_f64_workspace", m, d, dimb)
+        ws = workspace.get(wsb)
+        _lib.call("lddmm_moments_f64", ptr(src), m, d, ptr(w.contiguous()), dimb, ptr(c), ptr(out), ptr(ws), wsb,
+                  stream_handle())
+        h = out.cpu().numpy()
+        return h[:d * dimb].reshape(d, dimb), h[d * dimb:]
+
+    def _rows(self, u, c, W, b, f):
+        """f += (u - c) W + b on the device (lddmm_rows_affine_f64)."""
+        n, Q = u.shape
+        J = f.shape[1]
+        Wd = torch.from_numpy(np.ascontiguousarray(W, dtype=np.float64)).to(f.device)
+        bd = None if b is None else torch.from_numpy(np.ascontiguousarray(b, dtype=np.float64)).to(f.device)
+        _lib.call("lddmm_rows_affine_f64", ptr(u.contiguous()), n, Q, ptr(c) if c is not None else None, ptr(Wd),
+                  ptr(bd) if bd is not None else None, J, ptr(f), stream_handle())
+
+    def _affine_applyk(self, src, w, tgt, f):
+        d = src.shape[1]
+        if w.shape[1] > 4:
+            raise ValueError("affine kernel parts need at most 4 weight columns")
+        c = self._center_dev(d, src.device)
+        M, sums = self._moments(src, w, c)
+        if self.affine == 'affine':
+            # z += w1 (y - c) ((x - c)^T a) + w2 sum_l a_l
+            W = self.w1 * M
+        else:
+            if w.shape[1] != d:
+                raise ValueError("euclidean kernel parts need weights of the points' dimension")
+            # z += w2 sum_l a_l + w1 sum_E <(x - c) E^T, a> (y - c) E^T
+            W = np.zeros((d, d))
+            for E in self.affine_basis:
+                W += self.w1 * float((E * M.T).sum()) * E.T
+        self._rows(tgt, c, W, self.w2 * sums, f)
+
+    def _affine_difft(self, src, A1, A2, tgt, f):
+        if self.affine == 'affine':
+            # the reference's branch reads an undefined variable (kernelFunctions.py:437)
+            raise NotImplementedError("applyDiffKT of an 'affine' kernel fails in the reference "
+                                      "(kernelFunctions.py:437 uses an undefined `a`)")
+        na, _, d = A1.shape
+        c = self._center_dev(d, src.device)
+        # zpx += w1 sum_E sum_k <(x - c) E^T, a2[k]> a1[k] E
+        Bs = []
+        for k in range(na):
+            Mk, _ = self._moments(src, A2[k], c)
+            B = np.zeros((d, d))
+            for E in self.affine_basis:
+                B += float((E * Mk.T).sum()) * E
+            Bs.append(self.w1 * B)
+        step = max(1, 16 // d)
+        for k0 in range(0, na, step):
+            ks = list(range(k0, min(na, k0 + step)))
+            u = torch.cat([A1[k] for k in ks], dim=1)
+            self._rows(u, None, np.concatenate([Bs[k] for k in ks], axis=0), None, f)
 
     def applyDiffKT(self, x, a1, a2, firstVar=None):
         """sum_l grad_1 [a1_k . K(y_k, x_l) a2_l] (kernelFunctions.py:412-449)."""
@@ -119,6 +204,14 @@ class Kernel(KernelSpec):
         n, m, d = tgt.shape[0], src.shape[0], src.shape[1]
         if A1.shape[1] != n or A2.shape[1] != m:
             raise ValueError("applyDiffKT: a1 must cover the targets and a2 the sources")
+        if self.affine != 'none':
+            if self.affine == 'euclidean' and dimb != d:
+                raise ValueError("euclidean kernel parts need momenta of the points' dimension")
+            plain = self._plain()
+            f = to_dev(plain.applyDiffKT(src, A1, A2, firstVar=None if firstVar is None else tgt))
+            f = f.clone()
+            self._affine_difft(src, A1, A2, tgt, f)
+            return output_like(x, f)
         if self.name == 'none':
             return output_like(x, torch.zeros((n, d), dtype=torch.float64, device=src.device))
         f = torch.empty((n, d), dtype=torch.float64, device=src.device)
@@ -137,6 +230,12 @@ class Kernel(KernelSpec):
         _lib.call("lddmm_applykdifft_" + sfx, ptr(tgt), n, ptr(src), m, ptr(A1), ptr(A2), na, d, dimb,
                   float(self.sigma), int(self.order), ptr(f), ptr(ws), wsb, stream_handle())
         return output_like(x, f)
+
+    def _plain(self):
+        """The same kernel without its affine part."""
+        K = Kernel(name=self.name, sigma=self.sigma, order=self.order, weight=self.weight, precision=self.precision)
+        K.name = self.name
+        return K
 
     def applyDivergence(self, x, a, firstVar=None):
         """sum_l div_1 K(y_k, x_l) a_l, times KernelSpec.weight as the dense

@@ -119,10 +119,46 @@ def landmarkDirectEvolutionEuler(x0, at, KparDiff, affine=None, withJacobian=Fal
 
 
 def landmarkEPDiff(T, x0, a0, KparDiff, affine=None, withJacobian=False, withNormals=None, withPointSet=None):
-    """Momentum-carrying (EPDiff) shooting (pointEvolution.py:599-658); returns (xt, at)."""
+    """Momentum-carrying (EPDiff) shooting (pointEvolution.py:599-658); returns (xt, at), or
+    [xt, at, yt?, nt?, Jt?] with the optional outputs in the reference's order:
+      yt[k+1] = yt[k] + dt K(yt[k], x_k) a_k                        (withPointSet)
+      nt[k+1] = nt[k] - dt applyDiffKT(x_k, [nt[k]], [a_k])          (withNormals)
+      Jt[k+1] = Jt[k] + dt applyDivergence(x_k, a_k)                 (withJacobian; on the
+                points x, also with a point set, as in the reference: Jt is (T+1, N))"""
     _check_affine(affine)
-    if withJacobian or withNormals is not None or withPointSet is not None:
-        raise NotImplementedError("landmarkEPDiff optional outputs are not provided")
+    xt, at = _epdiff(T, x0, a0, KparDiff)
+    if not withJacobian and withNormals is None and withPointSet is None:
+        return output_like(x0, xt), output_like(x0, at)
+    timeStep = 1.0 / T
+    out = [xt, at]
+    if withPointSet is not None:
+        y0 = to_dev(withPointSet)
+        yt = torch.empty((T + 1,) + tuple(y0.shape), dtype=torch.float64, device=xt.device)
+        yt[0] = y0
+    if withNormals is not None:
+        nt = torch.empty_like(xt)
+        nt[0] = to_dev(withNormals)
+    if withJacobian:
+        Jt = torch.zeros((T + 1, xt.shape[1]), dtype=torch.float64, device=xt.device)
+    for k in range(T):
+        z, a = xt[k], at[k]
+        if withPointSet is not None:
+            yt[k + 1] = yt[k] + timeStep * KparDiff.applyK(z, a, firstVar=yt[k])
+        if withNormals is not None:
+            nt[k + 1] = nt[k] - timeStep * KparDiff.applyDiffKT(z, nt[k][None], a[None])
+        if withJacobian:
+            Jt[k + 1] = Jt[k] + timeStep * KparDiff.applyDivergence(z, a)
+    if withPointSet is not None:
+        out.append(yt)
+    if withNormals is not None:
+        out.append(nt)
+    if withJacobian:
+        out.append(Jt)
+    return [output_like(x0, t) for t in out]
+
+
+def _epdiff(T, x0, a0, KparDiff):
+    """The fused EPDiff operator (lddmm_epdiff_*): device (xt, at)."""
     require_cuda()
     x0d, a0d = to_dev(x0), to_dev(a0)
     n, d = x0d.shape
@@ -133,7 +169,7 @@ def landmarkEPDiff(T, x0, a0, KparDiff, affine=None, withJacobian=False, withNor
     ws = workspace.get(wsb)
     _lib.call("lddmm_epdiff_" + sfx, ptr(x0d), n, d, ptr(a0d), int(T), sigma, order, ptr(xt), ptr(at), ptr(ws), wsb,
               stream_handle())
-    return output_like(x0, xt), output_like(x0, at)
+    return xt, at
 
 
 def landmarkHamiltonianCovector(x0, at, px1, KparDiff, regweight, affine=None):

@@ -5,7 +5,7 @@ f2py Fortran module.  In this container there is neither a Python 2
 interpreter nor a Fortran compiler, so this script:
 
 1. loads the reference's own Python modules from the read-only reference
-   checkout (its py-lddmm/ directory, or $LDDMM_REFERENCE_DIR) after four
+   checkout (its py-lddmm/ directory, or $LDDMM_REFERENCE_DIR) after five
    mechanical, semantics-preserving source rewrites done in memory
    (nothing is copied into this repository):
      - tabs expanded to 8-column stops (Python 2 indentation rule);
@@ -14,6 +14,8 @@ interpreter nor a Fortran compiler, so this script:
        (what the comparison returned for arrays under the numpy of the
        Python 2 era; modern numpy compares element-wise instead);
      - ``len(x)/2`` turned into ``len(x)//2`` (Python 2 integer division);
+     - ``np.mat(`` turned into ``np.asmatrix(`` (the same function under the
+       name numpy 2 keeps);
 2. registers the oracle (``oracle.FortShim``, a C/OpenMP restatement of
    kernelFunctions.f90) as the module ``kernelFunctions_fort`` that the
    reference imports, and a stub ``gaussianDiffeons`` (imported by
@@ -29,6 +31,7 @@ optimisation state).  Run from the repository root:
 
     python tests/golden/make_golden.py              # both fixture files
     python tests/golden/make_golden.py --kff-calls  # tests/golden/kff_calls.npz only
+    python tests/golden/make_golden.py --extra      # tests/golden/reference_golden_extra.npz only
 """
 import io
 import os
@@ -61,6 +64,7 @@ def _py3_source(text):
         line = re.sub(r"!=\s*None\b", " is not None", line)
         line = re.sub(r"==\s*None\b", " is None", line)
         line = re.sub(r"(len\([^()]*\))/2\b", r"\1//2", line)
+        line = re.sub(r"\bnp\.mat\(", "np.asmatrix(", line)
         out.append(line)
     return "\n".join(out) + "\n"
 
@@ -520,6 +524,70 @@ def kff_call_cases(R):
     return out
 
 
+def extra_cases(R):
+    """Reference outputs of the options that the main fixtures do not cover:
+    landmarkEPDiff with a point set, normals and the Jacobian
+    (pointEvolution.py:599-658), and the affine / euclidean parts of
+    Kernel.applyK and the euclidean part of Kernel.applyDiffKT
+    (kernelFunctions.py:334-367, 431-448)."""
+    kf = R["kernelFunctions"]
+    ev = R["pointEvolution"]
+    out = {}
+    rng = np.random.default_rng(77)
+    for kname, sigma in [("gauss", 0.5), ("laplacian", 0.6)]:
+        N, d, T = 40, 3, 6
+        x0 = rng.uniform(-1, 1, (N, d))
+        a0 = 0.3 * rng.standard_normal((N, d))
+        grid = rng.uniform(-1, 1, (17, d))
+        n0 = rng.standard_normal((N, d))
+        K = kf.Kernel(name=kname, sigma=sigma)
+        xt, at, yt, nt, Jt = ev.landmarkEPDiff(T, x0, a0, K, withJacobian=True, withNormals=n0, withPointSet=grid)
+        xt2, at2, Jt2 = ev.landmarkEPDiff(T, x0, a0, K, withJacobian=True)
+        p = "epd_%s_" % kname
+        for k, v in dict(x0=x0, a0=a0, grid=grid, n0=n0, xt=xt, at=at, yt=yt, nt=nt, Jt=Jt, Jt_only=Jt2).items():
+            out[p + k] = v
+        out[p + "sigma"] = sigma
+    cases = []
+    for affine in ("affine", "euclidean"):
+        for d in (2, 3):
+            for kname in ("gauss", "laplacian"):
+                tag = "%s_%s_d%d" % (affine, kname, d)
+                n, m = 23, 31
+                x = rng.uniform(-1, 1, (m, d))    # sources
+                y = rng.uniform(-1, 1, (n, d))    # targets
+                a = rng.standard_normal((m, d))
+                K = kf.Kernel(name=kname, sigma=0.4, affine=affine, w1=0.7, w2=1.3, dim=d,
+                              center=list(rng.uniform(-0.2, 0.2, d)))
+                out["aff_x_" + tag], out["aff_y_" + tag], out["aff_a_" + tag] = x, y, a
+                out["aff_center_" + tag] = np.asarray(K.center, dtype=np.float64)
+                try:
+                    out["aff_k_" + tag] = K.applyK(x, a)
+                except ValueError:
+                    # euclidean, firstVar None: the reference multiplies np.matrix objects
+                    # ((xE * a).sum() is a matrix product, kernelFunctions.py:360) and fails
+                    pass
+                out["aff_kf_" + tag] = K.applyK(x, a, firstVar=y)
+                if affine == "euclidean":
+                    a1 = rng.standard_normal((2, n, d))
+                    a2 = rng.standard_normal((2, m, d))
+                    out["aff_a1_" + tag], out["aff_a2_" + tag] = a1, a2
+                    out["aff_dkt_" + tag] = K.applyDiffKT(x, a1, a2, firstVar=y)
+                    b1 = rng.standard_normal((1, m, d))
+                    b2 = rng.standard_normal((1, m, d))
+                    out["aff_b1_" + tag], out["aff_b2_" + tag] = b1, b2
+                    out["aff_dkts_" + tag] = K.applyDiffKT(x, b1, b2)
+                cases.append(tag)
+    out["aff_cases"] = np.array(cases)
+    return out
+
+
+def write_extra(R):
+    extra = extra_cases(R)
+    dst = os.path.join(HERE, "reference_golden_extra.npz")
+    np.savez_compressed(dst, **extra)
+    print("wrote %s (%d arrays, %.1f KB)" % (dst, len(extra), os.path.getsize(dst) / 1024.0))
+
+
 def write_kff_calls(R):
     calls = kff_call_cases(R)
     dst = os.path.join(HERE, "kff_calls.npz")
@@ -533,6 +601,9 @@ def main():
     R = load_reference()
     if "--kff-calls" in sys.argv:     # only the recorded kernelFunctions_fort calls
         write_kff_calls(R)
+        return
+    if "--extra" in sys.argv:         # only tests/golden/reference_golden_extra.npz
+        write_extra(R)
         return
     out = {}
     kernel_cases(R, out)
@@ -548,6 +619,7 @@ def main():
     np.savez_compressed(dst, **out)
     print("wrote %s (%d arrays, %.1f KB)" % (dst, len(out), os.path.getsize(dst) / 1024.0))
     write_kff_calls(R)
+    write_extra(R)
 
 
 if __name__ == "__main__":
