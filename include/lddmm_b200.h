@@ -133,6 +133,24 @@ LDDMM_API int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* 
                               double sigma, int order, double regweight, double* xt, double* energy,
                               void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
+/* The same shot along a search direction: the momenta are
+ *   at_try[t] = at[t] - (*eps) dir[t]   (eps: one double on the device)
+ * written to at_try (T, n, d), then shot as above.  No single counterpart in
+ * the reference: it is the trial step of SurfaceMatching / CurveMatching.updateTry
+ * (py-lddmm/surfaceMatching.py:255-289, curveMatching.py:185-208), atTry =
+ * at - eps dir followed by its objectiveFunDef shot, in one call whose eps
+ * lives on the device (a CUDA graph can replay it for every trial step).
+ * Same workspace as lddmm_shoot_*_workspace; the products and differences are
+ * rounded as two FP64 operations, as numpy's at - eps * dir. */
+LDDMM_API int lddmm_shoot_along_f32c(const double* x0, int64_t n, int d, const double* at, const double* dir,
+                                     const double* eps, int T, double dt, double sigma, int order, double regweight,
+                                     double* at_try, double* xt, double* energy, void* workspace,
+                                     size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API int lddmm_shoot_along_f64(const double* x0, int64_t n, int d, const double* at, const double* dir,
+                                    const double* eps, int T, double dt, double sigma, int order, double regweight,
+                                    double* at_try, double* xt, double* energy, void* workspace,
+                                    size_t workspace_bytes, lddmm_stream_t stream);
+
 /* ---- Hamiltonian adjoint: landmarkHamiltonianCovector / Gradient --------------
  * Replaces the backward loop of py-lddmm/pointEvolution.py:735-765 and the
  * gradient of :793-817 (no affine part), given the trajectory xt:

@@ -40,6 +40,8 @@ SIGNATURES = {
     "lddmm_shoot_f64_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_shoot_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _D, _I, _D, _P, _P, _P, _SZ, _P]),
     "lddmm_shoot_f64": (_I, [_P, _I64, _I, _P, _I, _D, _D, _I, _D, _P, _P, _P, _SZ, _P]),
+    "lddmm_shoot_along_f32c": (_I, [_P, _I64, _I, _P, _P, _P, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ, _P]),
+    "lddmm_shoot_along_f64": (_I, [_P, _I64, _I, _P, _P, _P, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ, _P]),
     "lddmm_covector_f32c_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_covector_f64_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_covector_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _P, _D, _I, _D, _P, _P, _P, _SZ, _P]),

@@ -188,8 +188,9 @@ class DeviceMatching:
         self.calls["updateTry"] += 1
         if self.cudaGraphs and self._fast_data:
             return self._graph_update_try(dir, eps, objRef)
-        atTry = self.at - eps * dir.diff
-        xt, e = evol.shoot(self.x0, atTry, self.param.KparDiff, regweight=self.regweight, with_energy=True)
+        eps_d = torch.full((), float(eps), dtype=torch.float64, device=self.x0.device)
+        atTry, xt, e = evol.shoot_along(self.x0, self.at, dir.diff, eps_d, self.param.KparDiff,
+                                        regweight=self.regweight)
         objTry = self._trial_value(e, xt[-1])
         if np.isnan(objTry):
             logging.info('Warning: nan in updateTry')
@@ -202,12 +203,11 @@ class DeviceMatching:
 
     # -- the trial step as one CUDA graph --------------------------------------------------
     def _trial_body(self):
-        """atTry = at - eps dir, its shot and its data-term value, on static buffers."""
+        """atTry = at - eps dir and its shot (one call), its data-term value, on static buffers."""
         g = self._graph
-        torch.sub(g["at"], torch.mul(g["dir"], g["eps"]), out=g["atTry"])
         out = g["out_buf"]   # [deformation energy, raw data term]: written in place by the two kernels
-        xt, _ = evol.shoot(self.x0, g["atTry"], self.param.KparDiff, regweight=self.regweight, with_energy=True,
-                           energy_out=out[0])
+        _, xt, _ = evol.shoot_along(self.x0, g["at"], g["dir"], g["eps"], self.param.KparDiff,
+                                    regweight=self.regweight, at_try=g["atTry"], energy_out=out[0])
         self._data_raw(xt[-1], out=out[1])
         return xt, out
 

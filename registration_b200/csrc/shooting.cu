@@ -186,7 +186,21 @@ struct ShootArgs {
     double rw;
     double* xt;
     double* energy;
+    // optional search direction: the shot's momenta are at - (*eps) dir, written to at_try
+    const double* dir = nullptr;
+    const double* eps = nullptr;
+    double* at_try = nullptr;
 };
+
+// at_try = at - (*eps) dir, rounded as two FP64 operations (the trial step of a line search)
+static __global__ void trial_momenta_kernel(const double* __restrict__ at, const double* __restrict__ dir,
+                                            const double* __restrict__ eps, long long count,
+                                            double* __restrict__ at_try) {
+    const double e = *eps;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        at_try[i] = __dsub_rn(at[i], __dmul_rn(e, dir[i]));
+}
 
 template <class Real, int KIND, int DEG, int D, bool SMALL = false>
 int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
@@ -238,11 +252,22 @@ int shoot_fused(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
     return launch_fused(shoot_fused_kernel<Real, KIND, DEG, D>, fs, fused_dyn_smem<Real>(a.n, D),
                         fused_dyn_smem<Real>(kFusedMaxPoints, 3), st, a.x0, a.at,
-                        (long long)a.n, a.T, dt, ks.scale, cf, a.rw, fs, a.xt, a.energy, epart);
+                        (long long)a.n, a.T, dt, ks.scale, cf, a.rw, fs, a.xt, a.energy, epart, a.dir, a.eps,
+                        a.at_try);
 }
 
 template <class Real>
-int shoot_run(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
+int shoot_run(const ShootArgs& a0, Workspace& ws, cudaStream_t st) {
+    ShootArgs a = a0;
+    if (a.dir != nullptr && !(a.n <= kFusedMaxPoints && a.d >= 2)) {
+        // general path: form the trial momenta, then shoot them
+        if (!ws.measuring()) {
+            const long long cnt = (long long)a.T * a.n * a.d;
+            trial_momenta_kernel<<<grid_for(cnt), 256, 0, st>>>(a.at, a.dir, a.eps, cnt, a.at_try);
+        }
+        a.at = a.at_try;
+        a.dir = nullptr;
+    }
     return dispatch_kind_p(a.order, [&](auto kind, auto deg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(deg)::value, D_ = decltype(D)::value;
@@ -615,6 +640,11 @@ int shoot_entry(const ShootArgs& a, void* wsp, size_t wsb, cudaStream_t st) {
     LDDMM_TRY(check_device_ptr(a.at, "at"));
     LDDMM_TRY(check_device_ptr(a.xt, "xt"));
     if (a.energy) LDDMM_TRY(check_device_ptr(a.energy, "energy"));
+    if (a.dir != nullptr || a.eps != nullptr || a.at_try != nullptr) {
+        LDDMM_TRY(check_device_ptr(a.dir, "dir"));
+        LDDMM_TRY(check_device_ptr(a.eps, "eps"));
+        LDDMM_TRY(check_device_ptr(a.at_try, "at_try"));
+    }
     return run_with_workspace([](const ShootArgs& q, Workspace& w, cudaStream_t s) { return shoot_run<Real>(q, w, s); },
                               a, wsp, wsb, st, "shoot");
 }
@@ -702,6 +732,26 @@ int lddmm_shoot_f64(const double* x0, int64_t n, int d, const double* at, int T,
                     int order, double regweight, double* xt, double* energy, void* workspace,
                     size_t workspace_bytes, lddmm_stream_t stream) {
     ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
+    return shoot_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int lddmm_shoot_along_f32c(const double* x0, int64_t n, int d, const double* at, const double* dir, const double* eps,
+                           int T, double dt, double sigma, int order, double regweight, double* at_try, double* xt,
+                           double* energy, void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
+    ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
+    a.dir = dir;
+    a.eps = eps;
+    a.at_try = at_try;
+    return shoot_entry<float>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int lddmm_shoot_along_f64(const double* x0, int64_t n, int d, const double* at, const double* dir, const double* eps,
+                          int T, double dt, double sigma, int order, double regweight, double* at_try, double* xt,
+                          double* energy, void* workspace, size_t workspace_bytes, lddmm_stream_t stream) {
+    ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
+    a.dir = dir;
+    a.eps = eps;
+    a.at_try = at_try;
     return shoot_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

@@ -60,6 +60,26 @@ def shoot(x0, at, KparDiff, regweight=1.0, with_energy=False, dt=None, energy_ou
     return xt, energy
 
 
+def shoot_along(x0, at, dir_, eps, KparDiff, regweight=1.0, at_try=None, energy_out=None):
+    """Device call: the shot of the trial momenta at - eps dir (eps a 0-d FP64 device
+    tensor), written to at_try (allocated if None); returns (at_try, xt, energy)."""
+    require_cuda()
+    x0d, atd, dd = to_dev(x0), to_dev(at), to_dev(dir_)
+    T, n, d = atd.shape
+    if dd.shape != atd.shape or x0d.shape != (n, d):
+        raise ValueError("x0 must be (N, dim), at and dir (T, N, dim)")
+    sigma, order, sfx = _kernel_args(KparDiff)
+    if at_try is None:
+        at_try = torch.empty_like(atd)
+    xt = torch.empty((T + 1, n, d), dtype=torch.float64, device=x0d.device)
+    energy = energy_out if energy_out is not None else torch.empty((), dtype=torch.float64, device=x0d.device)
+    wsb = _lib.query("lddmm_shoot_%s_workspace" % sfx, n, d, T)
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_shoot_along_" + sfx, ptr(x0d), n, d, ptr(atd), ptr(dd.contiguous()), ptr(eps), T, 0.0, sigma,
+              order, float(regweight), ptr(at_try), ptr(xt), ptr(energy), ptr(ws), wsb, stream_handle())
+    return at_try, xt, energy
+
+
 def covector(xt, at, px1, KparDiff, regweight, with_dat=True, dt=None):
     """Device call: returns (pxt, dat) given the trajectory xt (T+1, N, dim); dt defaults to 1/T."""
     require_cuda()
