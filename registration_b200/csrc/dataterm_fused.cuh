@@ -1,4 +1,7 @@
-// Single-launch data-term value for small shapes (at most kFusedMaxCells cells).
+// Single-launch data-term value for small shapes (at most kFusedMaxCells cells,
+// and at most kFusedMaxCells * 2 kFusedMaxCells cell pairs: beyond that the
+// pair sums keep the cluster's SMs busy for longer than the general path's
+// launches over all SMs take; measured crossover about 512 cells per shape).
 //
 // NormDef (or Norm0 with no target cells) of the current / measure / varifold
 // data terms (py-lddmm/surfaces.py:1009-1221, curves.py:539-650) in one
@@ -27,7 +30,10 @@
 
 namespace lddmm {
 
-constexpr long long kFusedMaxCells = 1024;
+#ifndef LDDMM_FUSED_MAX_CELLS
+#define LDDMM_FUSED_MAX_CELLS 512
+#endif
+constexpr long long kFusedMaxCells = LDDMM_FUSED_MAX_CELLS;
 
 template <class Real>
 struct DtTile {

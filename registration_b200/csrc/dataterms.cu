@@ -162,7 +162,7 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     return cuda_check(cudaGetLastError(), "dataterm");
 }
 
-// Values alone of at most kFusedMaxCells cells: one cluster launch (dataterm_fused.cuh).
+// Values alone of small shapes (dataterm_fused.cuh limits): one cluster launch.
 template <class Real, int KIND, int PDEG, int D>
 int dt_value_fused(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     const FusedShape fs = fused_shape(a.nc);
@@ -183,7 +183,8 @@ int dt_run(const DataArgs& a, Workspace& ws, cudaStream_t st) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(pdeg)::value, Q_ = decltype(qdeg)::value,
                           D_ = decltype(D)::value;
-            if (a.px == nullptr && a.energy != nullptr && a.nc <= kFusedMaxCells && a.d == D_)
+            if (a.px == nullptr && a.energy != nullptr && a.nc <= kFusedMaxCells &&
+                a.nc * (a.nc + a.nc2) <= 2 * kFusedMaxCells * kFusedMaxCells && a.d == D_)
                 return dt_value_fused<Real, K_, P_, D_>(a, ws, st);
             if (a.nc <= kSmallTargets) return dt_impl<Real, K_, P_, Q_, D_, true>(a, ws, st);
             return dt_impl<Real, K_, P_, Q_, D_>(a, ws, st);

@@ -6,14 +6,19 @@
 // kernel on one thread-block cluster of C <= 8 CTAs instead of a sweep and a
 // combine launch per step (plus bounding-box and pack launches): at a few
 // hundred points every launch is a few microseconds of mostly idle GPU.
+// Beyond about 512 points the n^2 pair sums of a step keep the cluster's 8
+// SMs busy for longer than the general path's launches over all SMs take
+// (measured on B200 at T = 10: 59 vs 82 us per shot at 512 points, 120 vs
+// 89 us at 768), so the limit is 512.
 //
 // Work split: C = min(8, ceil(n / 32)) CTAs; CTA r of the cluster owns the
-// targets [r*nc, (r+1)*nc), nc = ceil(n / C) <= 128.  Its 256 threads are tpt target slots (tpt = the next
-// power of two >= nc) times S = 256 / tpt source groups; group g sums the
-// sources [g*n/S, (g+1)*n/S) of its target (FP32 partials over 32 sources
-// folded into TwoSum pairs, or plain FP64), and the S group sums of a target
-// are added in group order in FP64.  Every result is a function of the shape
-// and the data only (no atomics), so repeated calls are bit-identical.
+// targets [r*nc, (r+1)*nc), nc = ceil(n / C) <= 64.  Its 512 threads are tpt
+// target slots (tpt = the next power of two >= nc) times S = 512 / tpt source
+// groups; group g sums the sources [g*n/S, (g+1)*n/S) of its target (FP32
+// partials over 32 sources folded into TwoSum pairs, or plain FP64), and the
+// S group sums of a target are added in group order in FP64.  Every result is
+// a function of the shape and the data only (no atomics), so repeated calls
+// are bit-identical.
 //
 // Step t: every CTA sums over the n source records (position in the packing
 // frame, weights) of the step held in its shared memory; the slot-0 thread of
@@ -39,17 +44,20 @@
 namespace lddmm {
 
 #ifndef LDDMM_FUSED_THREADS
-#define LDDMM_FUSED_THREADS 256
+#define LDDMM_FUSED_THREADS 512
 #endif
 #ifndef LDDMM_FUSED_UNROLL
 #define LDDMM_FUSED_UNROLL 1
 #endif
 constexpr int kFusedThreads = LDDMM_FUSED_THREADS;
 constexpr int kFusedUnroll = LDDMM_FUSED_UNROLL;   // inner source loop
-constexpr long long kFusedMaxPoints = 1024;
+#ifndef LDDMM_FUSED_MAX_POINTS
+#define LDDMM_FUSED_MAX_POINTS 512
+#endif
+constexpr long long kFusedMaxPoints = LDDMM_FUSED_MAX_POINTS;
 constexpr int kFusedMaxCluster = 8;
 // targets per CTA before the cluster grows: every CTA of a full cluster then
-// owns <= 128 targets, each target spread over >= 2 source groups
+// owns <= 64 targets, each target spread over >= 8 source groups
 constexpr int kFusedTargetsPerCta = 32;
 
 struct FusedShape {
@@ -219,120 +227,6 @@ LDDMM_D void fused_broadcast(const FusedRec<Real>& r, FusedRec<Real>* slot, int 
     }
 }
 
-// Step synchronisation with transaction barriers (LDDMM_FUSED_MBAR = 1): each
-// CTA keeps one mbarrier per record buffer; the owner of each target writes its
-// next-step record into every CTA with st.async ... mbarrier::complete_tx, so
-// the consumer waits only for the bytes of that step (n records) to land, and
-// no cluster-wide barrier (with its release fence) sits between two steps.
-// Buffer b's barrier is armed (arrive.expect_tx) for step s + 2 right after
-// its wait for step s: remote writes for step s + 2 need this CTA's step-(s+1)
-// records, sent after that point, so the transaction count never runs ahead.
-// Waits are bounded (one second of the global timer, and a poll count); a CTA
-// that gives up records the failure, stops waiting and arming, and the kernel
-// writes NaN results instead of hanging.
-#ifndef LDDMM_FUSED_MBAR
-#define LDDMM_FUSED_MBAR 0
-#endif
-constexpr long long kMbarPolls = 1LL << 26;
-constexpr unsigned long long kMbarWaitNs = 1000000000ULL;
-
-LDDMM_D unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-LDDMM_D unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-LDDMM_D void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-LDDMM_D void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-LDDMM_D void mbar_arm(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-// true when the phase of parity `parity` has completed (bounded number of polls)
-LDDMM_D bool mbar_wait(unsigned long long* bar, unsigned parity) {
-    const unsigned a = smem_addr(bar);
-    const unsigned long long t0 = global_ns();
-    for (long long it = 0; it < kMbarPolls; ++it) {
-        if ((it & 255) == 255 && global_ns() - t0 > kMbarWaitNs) return false;
-        unsigned done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-// the record `r` into slot `slot` of every CTA, completing `bar` (same offset in every CTA)
-template <class Real>
-LDDMM_D void fused_broadcast_async(const FusedRec<Real>& r, FusedRec<Real>* slot, unsigned long long* bar, int C) {
-    constexpr int W = sizeof(FusedRec<Real>) / 16;
-    const uint4* src = reinterpret_cast<const uint4*>(&r);
-    const unsigned laddr = smem_addr(slot), lbar = smem_addr(bar);
-    for (int q = 0; q < C; ++q) {
-        unsigned raddr, rbar;
-        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(raddr) : "r"(laddr), "r"(q));
-        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rbar) : "r"(lbar), "r"(q));
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-            const uint4 v = src[w];
-            asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];"
-                         ::"r"(raddr + 16 * w), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(rbar)
-                         : "memory");
-        }
-    }
-}
-
-// Per-CTA step synchronisation of the fused kernels: wait(s) before reading
-// the records of step s (s >= 1), publish(...) to send a record for step s + 1.
-template <class Real>
-struct FusedSteps {
-    unsigned long long* bar;   // [2], shared
-    int* failed;               // shared flag
-    unsigned uses[2];
-    unsigned bytes;
-    int T;
-    LDDMM_D void init(unsigned long long* b, int* f, long long n, int T_) {
-        bar = b;
-        failed = f;
-        uses[0] = uses[1] = 0;
-        bytes = (unsigned)(n * sizeof(FusedRec<Real>));
-        T = T_;
-        if (LDDMM_FUSED_MBAR && threadIdx.x == 0) {
-            *failed = 0;
-            mbar_init(&bar[0], 1);
-            mbar_init(&bar[1], 1);
-            mbar_fence_init();
-            if (T > 1) mbar_arm(&bar[1], bytes);   // step 1
-        }
-    }
-    // start of step s: the records of step s are in buffer s & 1
-    LDDMM_D void wait(int s) {
-        if (!LDDMM_FUSED_MBAR) return;
-        const int b = s & 1;
-        if (s > 0 && *(volatile int*)failed == 0) {
-            if (!mbar_wait(&bar[b], uses[b] & 1)) atomicOr(failed, 1);
-            ++uses[b];
-        }
-        if (threadIdx.x == 0 && s + 2 < T && *(volatile int*)failed == 0) mbar_arm(&bar[b], bytes);
-    }
-    LDDMM_D void publish(const FusedRec<Real>& r, FusedRec<Real>* slot, int s_next, int C) {
-        if (LDDMM_FUSED_MBAR) fused_broadcast_async<Real>(r, slot, &bar[s_next & 1], C);
-        else fused_broadcast<Real>(r, slot, C);
-    }
-    // end of a step: shared scratch reuse (and, without transaction barriers, the cluster barrier)
-    LDDMM_D void end_step() {
-        if (LDDMM_FUSED_MBAR) __syncthreads();
-        else cluster_sync_acq_rel();
-    }
-};
-
 // ---- shooting: xt[t+1] = xt[t] + dt K(xt[t]) at[t]; energy = rw dt sum_t <at[t], K at[t]> ----
 // Source records are double-buffered: step t reads buffer t & 1, and the owner
 // of each target writes its step-(t+1) record into buffer (t+1) & 1 of every
@@ -378,18 +272,12 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
     double xk64[3] = {0, 0, 0};
     if (owner && g == 0)
         for (int j = 0; j < D; ++j) xk64[j] = x0[k * D + j];
-    __shared__ unsigned long long step_bar[2];
-    __shared__ int step_failed;
-    FusedSteps<Real> steps;
-    steps.init(step_bar, &step_failed, n, T);
-    // every CTA's buffer 0 is complete (and its barriers initialised) before any
-    // CTA's owners write into its buffer 1
+    // every CTA's buffer 0 is complete before any CTA's owners overwrite its buffer 1
     cluster_sync_acq_rel();
     double e_acc = 0.0;
     for (int t = 0; t < T; ++t) {
         const FusedRec<Real>* rec = (t & 1) ? rec1 : rec0;
         FusedRec<Real>* nxt = (t & 1) ? rec0 : rec1;
-        steps.wait(t);
         // slot 0: store the row x_t of the output (off the critical path: the next cluster
         // barrier's release is a step away) and prefetch the momenta the update needs
         double a_now[3] = {0, 0, 0}, a_next[3] = {0, 0, 0};
@@ -441,22 +329,22 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
             if (t + 1 < T) {
                 FusedRec<Real> r;
                 fused_store<Real>(r, xk64, D, scale, c, a_next, D);
-                steps.publish(r, nxt + k, t + 1, fs.C);
+                fused_broadcast<Real>(r, nxt + k, fs.C);
             }
         }
-        steps.end_step();
+        cluster_sync_acq_rel();
     }
-    const bool bad = LDDMM_FUSED_MBAR && step_failed != 0;
     if (owner && g == 0)
-        for (int j = 0; j < D; ++j) xt[(long long)T * N + k * D + j] = bad ? NAN : xk64[j];
-    const double e = fused_block_sum(bad ? NAN : e_acc, scratch);
-    if (tid == 0) __stcg(epart + rank, e);
-    // no CTA leaves while another may still write into its shared memory
-    cluster_sync_acq_rel();
-    if (energy != nullptr && rank == 0 && tid == 0) {
-        double sum = 0.0;
-        for (int r = 0; r < fs.C; ++r) sum += __ldcg(epart + r);
-        energy[0] = rw * dt * sum;
+        for (int j = 0; j < D; ++j) xt[(long long)T * N + k * D + j] = xk64[j];
+    if (energy != nullptr) {
+        const double e = fused_block_sum(e_acc, scratch);
+        if (tid == 0) __stcg(epart + rank, e);
+        cluster_sync_acq_rel();
+        if (rank == 0 && tid == 0) {
+            double sum = 0.0;
+            for (int r = 0; r < fs.C; ++r) sum += __ldcg(epart + r);
+            energy[0] = rw * dt * sum;
+        }
     }
 }
 
@@ -507,10 +395,6 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
             pxt[(long long)T * N + k * D + j] = pn[j];
             pown[local * 3 + j] = pn[j];
         }
-    __shared__ unsigned long long step_bar[2];
-    __shared__ int step_failed;
-    FusedSteps<Real> steps;
-    steps.init(step_bar, &step_failed, n, T);
     cluster_sync_acq_rel();
     // slot 0 stores step t's rows of pxt and dat at the start of step t - 1 (off the
     // critical path: the release of the next cluster barrier is a step away)
@@ -529,8 +413,6 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
         const FusedRec<Real>* rec = b ? rec1 : rec0;
         FusedRec<Real>* nxt = b ? rec0 : rec1;
         const double* as = at + (long long)t * N;
-        const int s = T - 1 - t;   // step index: the records of step s are in buffer s & 1
-        steps.wait(s);
         if (owner && g == 0) flush();
         if (owner) {
             Real xk[3], u[6];
@@ -585,7 +467,7 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
                 }
                 FusedRec<Real> r;
                 fused_store<Real>(r, xt + (long long)(t - 1) * N + k * D, D, scale, c, v, 2 * D);
-                steps.publish(r, nxt + k, s + 1, fs.C);
+                fused_broadcast<Real>(r, nxt + k, fs.C);
             }
             for (int q = 0; q < D; ++q) {
                 pend_d[q] = 2.0 * rw * as[k * D + q] - pn[q];
@@ -595,19 +477,9 @@ __global__ void __launch_bounds__(kFusedThreads) cov_fused_kernel(const double* 
             }
             pend = t;
         }
-        steps.end_step();
-    }
-    if (owner && g == 0) flush();
-    if (LDDMM_FUSED_MBAR) {
-        if (step_failed != 0 && owner && g == 0)
-            for (int t = 0; t <= T; ++t)
-                for (int q = 0; q < D; ++q) {
-                    pxt[(long long)t * N + k * D + q] = NAN;
-                    if (dat != nullptr && t < T) dat[(long long)t * N + k * D + q] = NAN;
-                }
-        // no CTA leaves while another may still write into its shared memory
         cluster_sync_acq_rel();
     }
+    if (owner && g == 0) flush();
 }
 
 template <class Real>
