@@ -151,6 +151,32 @@ LDDMM_API int lddmm_shoot_along_f64(const double* x0, int64_t n, int d, const do
                                     double* at_try, double* xt, double* energy, void* workspace,
                                     size_t workspace_bytes, lddmm_stream_t stream);
 
+/* A batch of trial steps along one direction: step sizes eps[0..nbatch) on
+ * the device, outputs stacked per step size: at_try (nbatch, T, n, d), xt
+ * (nbatch, T+1, n, d), energy (nbatch) (may be NULL).  Slot b equals, bit for
+ * bit, lddmm_shoot_along_* with eps[b].  No counterpart in the reference: the
+ * step sizes cg's line search tries next (eps / 2^k while halving, eps 1.25^j
+ * while growing; conjugateGradient.py:140-183) are shot side by side, one
+ * thread-block cluster each, when the point set is small enough for a cluster
+ * to leave most SMs idle (lddmm_trial_batch_size > 1); otherwise one after the
+ * other.  1 <= nbatch <= 4096. */
+LDDMM_API size_t lddmm_shoot_along_batch_f32c_workspace(int64_t n, int d, int T, int nbatch);
+LDDMM_API int lddmm_shoot_along_batch_f32c(const double* x0, int64_t n, int d, const double* at, const double* dir,
+                                           const double* eps, int nbatch, int T, double dt, double sigma, int order,
+                                           double regweight, double* at_try, double* xt, double* energy,
+                                           void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API size_t lddmm_shoot_along_batch_f64_workspace(int64_t n, int d, int T, int nbatch);
+LDDMM_API int lddmm_shoot_along_batch_f64(const double* x0, int64_t n, int d, const double* at, const double* dir,
+                                          const double* eps, int nbatch, int T, double dt, double sigma, int order,
+                                          double regweight, double* at_try, double* xt, double* energy,
+                                          void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+
+/* How many trial steps of a problem (n points in d dimensions, a data term of
+ * nc own and nc2 target cells) one batched launch runs side by side: 1 when the
+ * batch would run one step size after the other (the general path), else up
+ * to 16, bounded by the SMs over the cluster size. */
+LDDMM_API int lddmm_trial_batch_size(int64_t n, int d, int64_t nc, int64_t nc2);
+
 /* ---- Hamiltonian adjoint: landmarkHamiltonianCovector / Gradient --------------
  * Replaces the backward loop of py-lddmm/pointEvolution.py:735-765 and the
  * gradient of :793-817 (no affine part), given the trajectory xt:
@@ -214,6 +240,28 @@ LDDMM_API int lddmm_dataterm_f64(int cell_size, int norm, const double* vertices
                                  const double* tgt_vectors, int64_t nc2, double sigma, int order, double eps1,
                                  double eps2, double* energy, const int64_t* vertex_ptr, const int64_t* vertex_idx,
                                  double* px, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+
+/* Values of a batch of vertex sets of the same shape (the final positions of
+ * batched trial steps): vertex set b starts at vertices + b vertex_stride
+ * (vertex_stride >= nv d), energy[b] as lddmm_dataterm_* with px NULL, bit for
+ * bit.  One cluster per vertex set side by side for small shapes, else one
+ * after the other.  1 <= nbatch <= 4096. */
+LDDMM_API size_t lddmm_dataterm_value_batch_f32c_workspace(int cell_size, int norm, int64_t nv, int d, int64_t nc,
+                                                           int64_t nc2, int order, int nbatch);
+LDDMM_API int lddmm_dataterm_value_batch_f32c(int cell_size, int norm, const double* vertices, int64_t nv, int d,
+                                              const int64_t* cells, int64_t nc, const double* tgt_centers,
+                                              const double* tgt_vectors, int64_t nc2, double sigma, int order,
+                                              double eps1, double eps2, int nbatch, int64_t vertex_stride,
+                                              double* energy, void* workspace, size_t workspace_bytes,
+                                              lddmm_stream_t stream);
+LDDMM_API size_t lddmm_dataterm_value_batch_f64_workspace(int cell_size, int norm, int64_t nv, int d, int64_t nc,
+                                                          int64_t nc2, int order, int nbatch);
+LDDMM_API int lddmm_dataterm_value_batch_f64(int cell_size, int norm, const double* vertices, int64_t nv, int d,
+                                             const int64_t* cells, int64_t nc, const double* tgt_centers,
+                                             const double* tgt_vectors, int64_t nc2, double sigma, int order,
+                                             double eps1, double eps2, int nbatch, int64_t vertex_stride,
+                                             double* energy, void* workspace, size_t workspace_bytes,
+                                             lddmm_stream_t stream);
 
 /* ---- dense-weight kernel sums: kff.applykmat / kff.applykdiffmat ---------------
  * Replace py-lddmm/kernelFunctions.f90:499-552 and :554-610 (called by

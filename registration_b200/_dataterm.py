@@ -92,3 +92,39 @@ def dataterm(norm, vertices, dshape, tgt_centers, tgt_vectors, K, energy=True, g
               int(K.order), float(eps1), float(eps2), ptr(e) if e is not None else None, ptr(dshape.vptr),
               ptr(dshape.vidx), ptr(px) if px is not None else None, ptr(ws), wsb, stream_handle())
     return e, px
+
+
+def value_batch(norm, vertices, dshape, tgt_centers, tgt_vectors, K, eps1=1e-10, eps2=1e-10, energy_out=None):
+    """Values (nbatch,) of the vertex sets vertices[b] of one topology `dshape`
+    against one target: vertices is an (nbatch, nv, d) FP64 device view whose
+    vertex sets are contiguous (any stride between them, e.g. xt[:, -1] of
+    batched trajectories); energy_out: a contiguous (nbatch,) FP64 device tensor.
+    energy[b] is bit-identical to dataterm(norm, vertices[b], ...)."""
+    require_cuda()
+    if K.name == 'none':
+        raise ValueError("a kernel is required")
+    v = vertices
+    if not (isinstance(v, torch.Tensor) and v.is_cuda and v.dtype == torch.float64 and v.dim() == 3):
+        raise ValueError("vertices must be an (nbatch, nv, d) FP64 device tensor")
+    B, nv, d = v.shape
+    if v.stride(2) != 1 or v.stride(1) != d or (B > 1 and v.stride(0) < nv * d):
+        raise ValueError("each vertex set must be contiguous and the sets must not overlap")
+    k = dshape.cells.shape[1]
+    nc = dshape.cells.shape[0]
+    if tgt_centers is None:
+        c2 = s2 = None
+        nc2 = 0
+    else:
+        c2, s2 = to_dev(tgt_centers), to_dev(tgt_vectors)
+        nc2 = c2.shape[0]
+    sfx = _suffix(K.precision)
+    e = energy_out if energy_out is not None else torch.empty(B, dtype=torch.float64, device=v.device)
+    if tuple(e.shape) != (B,) or not e.is_contiguous():
+        raise ValueError("energy_out must be a contiguous (nbatch,) tensor")
+    wsb = _lib.query("lddmm_dataterm_value_batch_%s_workspace" % sfx, k, NORMS[norm], nv, d, nc, nc2, int(K.order), B)
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_dataterm_value_batch_" + sfx, k, NORMS[norm], ptr(v), nv, d, ptr(dshape.cells), nc,
+              ptr(c2) if c2 is not None else None, ptr(s2) if s2 is not None else None, nc2, float(K.sigma),
+              int(K.order), float(eps1), float(eps2), B, v.stride(0) if B > 1 else nv * d, ptr(e), ptr(ws), wsb,
+              stream_handle())
+    return e

@@ -42,6 +42,13 @@ SIGNATURES = {
     "lddmm_shoot_f64": (_I, [_P, _I64, _I, _P, _I, _D, _D, _I, _D, _P, _P, _P, _SZ, _P]),
     "lddmm_shoot_along_f32c": (_I, [_P, _I64, _I, _P, _P, _P, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ, _P]),
     "lddmm_shoot_along_f64": (_I, [_P, _I64, _I, _P, _P, _P, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ, _P]),
+    "lddmm_shoot_along_batch_f32c_workspace": (_SZ, [_I64, _I, _I, _I]),
+    "lddmm_shoot_along_batch_f64_workspace": (_SZ, [_I64, _I, _I, _I]),
+    "lddmm_shoot_along_batch_f32c": (_I, [_P, _I64, _I, _P, _P, _P, _I, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ,
+                                          _P]),
+    "lddmm_shoot_along_batch_f64": (_I, [_P, _I64, _I, _P, _P, _P, _I, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ,
+                                         _P]),
+    "lddmm_trial_batch_size": (_I, [_I64, _I, _I64, _I64]),
     "lddmm_covector_f32c_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_covector_f64_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_covector_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _P, _D, _I, _D, _P, _P, _P, _SZ, _P]),
@@ -52,6 +59,12 @@ SIGNATURES = {
                                  _P, _SZ, _P]),
     "lddmm_dataterm_f64": (_I, [_I, _I, _P, _I64, _I, _P, _I64, _P, _P, _I64, _D, _I, _D, _D, _P, _P, _P, _P,
                                 _P, _SZ, _P]),
+    "lddmm_dataterm_value_batch_f32c_workspace": (_SZ, [_I, _I, _I64, _I, _I64, _I64, _I, _I]),
+    "lddmm_dataterm_value_batch_f64_workspace": (_SZ, [_I, _I, _I64, _I, _I64, _I64, _I, _I]),
+    "lddmm_dataterm_value_batch_f32c": (_I, [_I, _I, _P, _I64, _I, _P, _I64, _P, _P, _I64, _D, _I, _D, _D, _I, _I64,
+                                             _P, _P, _SZ, _P]),
+    "lddmm_dataterm_value_batch_f64": (_I, [_I, _I, _P, _I64, _I, _P, _I64, _P, _P, _I64, _D, _I, _D, _D, _I, _I64,
+                                            _P, _P, _SZ, _P]),
     "lddmm_epdiff_f32c_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_epdiff_f64_workspace": (_SZ, [_I64, _I, _I]),
     "lddmm_epdiff_f32c": (_I, [_P, _I64, _I, _P, _I, _D, _I, _P, _P, _P, _SZ, _P]),

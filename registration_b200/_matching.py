@@ -201,28 +201,66 @@ class DeviceMatching:
             self.xtTry = xt
         return objTry
 
-    # -- the trial step as one CUDA graph --------------------------------------------------
+    # -- the trial steps as one CUDA graph --------------------------------------------------
     def _trial_body(self):
-        """atTry = at - eps dir and its shot (one call), its data-term value, on static buffers."""
+        """For every step size of g["eps"]: atTry = at - eps dir, its shot and its
+        data-term value, on static buffers (one cluster per step size when the
+        problem is small, so a batch costs about what one trial step does)."""
         g = self._graph
-        out = g["out_buf"]   # [deformation energy, raw data term]: written in place by the two kernels
-        _, xt, _ = evol.shoot_along(self.x0, g["at"], g["dir"], g["eps"], self.param.KparDiff,
-                                    regweight=self.regweight, at_try=g["atTry"], energy_out=out[0])
-        self._data_raw(xt[-1], out=out[1])
-        return xt, out
+        out = g["out_buf"]   # [deformation energies, raw data terms] (2, B): written in place
+        _, xt, _ = evol.shoot_along_batch(self.x0, g["at"], g["dir"], g["eps"], self.param.KparDiff,
+                                          regweight=self.regweight, at_try=g["atTry"], xt=g["xt"],
+                                          energy=out[0])
+        _dt.value_batch(self.param.errorType, xt[:, -1], self._dshape, self._tc, self._tv, self._Kval,
+                        energy_out=out[1])
+        return out
+
+    def expectTrials(self, dir, steps):
+        """Optional line-search hint: the step sizes `steps` along `dir` that the
+        next updateTry calls may ask for besides the halving and growth ladders
+        (cg's tiny-step probe).  Changes no value, only what a batch holds."""
+        self._hint = (dir.diff, [float(e) for e in steps])
+
+    def _trial_ladder(self, eps, cache, dir_diff):
+        """The step sizes to evaluate with `eps`: the ones cg tries next from it
+        (conjugateGradient.py:140-183), computed with cg's own operations so
+        that they compare equal: eps 1.25^j (chained) when eps is a growth step
+        of an evaluated size, else eps / 2^k (the halving loops) and the hinted
+        steps of this direction."""
+        B = self._graph["B"]
+        if B == 1:
+            return [eps]
+        hint = getattr(self, "_hint", None)
+        extra = [e for e in hint[1] if e != eps] if hint is not None and hint[0] is dir_diff else []
+        grow = any(1.25 * e == eps for e in cache)
+        if grow:
+            extra = []
+        ladder = [eps]
+        while len(ladder) < B - len(extra):
+            ladder.append(1.25 * ladder[-1] if grow else ladder[-1] / 2)
+        return ladder + [e for e in extra if e not in ladder][:B - len(ladder)]
 
     def _graph_update_try(self, dir, eps, objRef):
-        """updateTry with the shot and the data-term value replayed from a CUDA
-        graph captured on the first call: the same kernels on the same inputs
-        (bit-identical to the eager path), one launch from the host, one read
-        back.  The static copies of `at` and of the direction are refreshed
-        only when cg hands over new tensors."""
+        """updateTry with the trial steps replayed from a CUDA graph captured on
+        the first call: the same kernels on the same inputs (bit-identical to
+        the eager path), one launch and one read-back per batch of step sizes.
+        A batch evaluates the step sizes the line search asks for next along the
+        same direction; later calls for them are answered from it until the
+        momenta or the direction change.  The static copies of `at` and of the
+        direction are refreshed only when cg hands over new tensors."""
         g = self._graph
         if g is None:
-            g = self._graph = {"at": self.at.clone(), "dir": dir.diff.clone(),
-                               "eps": torch.full((), float(eps), dtype=torch.float64, device=self.x0.device),
-                               "atTry": torch.empty_like(self.at), "at_src": self.at, "dir_src": dir.diff,
-                               "out_buf": torch.empty(2, dtype=torch.float64, device=self.x0.device)}
+            dev = self.x0.device
+            B = evol.trial_batch_size(self.npt, self.dim, self._dshape.cells.shape[0], self._tc.shape[0])
+            T, n, d = self.at.shape
+            g = self._graph = {"B": B, "at": self.at.clone(), "dir": dir.diff.clone(),
+                               "eps": torch.full((B,), float(eps), dtype=torch.float64, device=dev),
+                               "atTry": torch.empty((B, T, n, d), dtype=torch.float64, device=dev),
+                               "xt": torch.empty((B, T + 1, n, d), dtype=torch.float64, device=dev),
+                               "out_buf": torch.empty((2, B), dtype=torch.float64, device=dev),
+                               "eps_host": torch.empty(B, dtype=torch.float64).pin_memory(),
+                               "out_host": torch.empty((2, B), dtype=torch.float64).pin_memory(),
+                               "at_src": self.at, "dir_src": dir.diff, "cache": {}}
             # capture on a side stream with the low-level calls (the torch.cuda.graph
             # context manager also collects garbage and empties the allocator cache)
             side = torch.cuda.Stream()
@@ -234,7 +272,7 @@ class DeviceMatching:
                 with workspace.scope(self):
                     graph.capture_begin()
                     try:
-                        g["xt"], g["out"] = self._trial_body()
+                        self._trial_body()
                     finally:
                         graph.capture_end()
             torch.cuda.current_stream().wait_stream(side)
@@ -242,23 +280,36 @@ class DeviceMatching:
         if g["at_src"] is not self.at:
             g["at"].copy_(self.at)
             g["at_src"] = self.at
+            g["cache"] = {}
         if g["dir_src"] is not dir.diff:
             g["dir"].copy_(dir.diff)
             g["dir_src"] = dir.diff
-        g["eps"].fill_(float(eps))
-        g["graph"].replay()
-        host = g["out"].cpu().numpy()
-        ereg = float(host[0])
-        objTry = self._combine(ereg, float(host[1]))
+            g["cache"] = {}
+        cache = g["cache"]
+        eps = float(eps)
+        if eps not in cache:
+            ladder = self._trial_ladder(eps, cache, dir.diff)
+            g["eps_host"].numpy()[:] = ladder
+            g["eps"].copy_(g["eps_host"], non_blocking=True)
+            g["graph"].replay()
+            self.calls["trial_batches"] = self.calls.get("trial_batches", 0) + 1
+            g["out_host"].copy_(g["out_buf"], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            host = g["out_host"].numpy()
+            cache.clear()
+            for b, e in enumerate(ladder):
+                cache.setdefault(e, (b, float(host[0, b]), float(host[1, b])))
+        b, ereg, raw = cache[eps]
+        objTry = self._combine(ereg, raw)
         if self._auto:
-            objTry = _Value(objTry, self, ereg, g["xt"][-1].clone(), value_bound(self, self._noise, self.obj0))
+            objTry = _Value(objTry, self, ereg, g["xt"][b, -1].clone(), value_bound(self, self._noise, self.obj0))
         if np.isnan(objTry):
             logging.info('Warning: nan in updateTry')
             return 1e500
         if (objRef is None) or (objTry < objRef):
-            self.atTry = g["atTry"].clone()
+            self.atTry = g["atTry"][b].clone()
             self.objTry = objTry
-            self.xtTry = g["xt"].clone()
+            self.xtTry = g["xt"][b].clone()
         return objTry
 
     def getGradient(self, coeff=1.0):

@@ -74,10 +74,15 @@ def cg(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=10.):
             dir0 = opt.addProd(grd, oldDir, beta) if hasattr(opt, 'addProd') else grd + beta * oldDir
             oldDir = copy(dir0)
             grdOld = copy(grd)
+        epsSmall = 0.000001 / grdTry
+        if hasattr(opt, 'expectTrials'):
+            # optional hint (no counterpart in the reference): the tiny-step probe
+            # below may follow, so an optimiser that evaluates step sizes in
+            # batches can include it; no decision depends on it
+            opt.expectTrials(dir0, [eps, epsSmall])
         objTry = opt.updateTry(dir0, eps, obj)
         noUpdate = 0
         if objTry > obj:
-            epsSmall = 0.000001 / grdTry
             objTry0 = opt.updateTry(dir0, epsSmall, obj)
             if objTry0 > obj:
                 if (skipCG == 1) | (beta < 1e-10):

@@ -35,6 +35,15 @@ namespace lddmm {
 #endif
 constexpr long long kFusedMaxCells = LDDMM_FUSED_MAX_CELLS;
 
+// a value of nc own cells against nc2 target cells runs as one cluster launch
+inline bool dt_fused_fits(long long nc, long long nc2) {
+    return nc >= 1 && nc <= kFusedMaxCells && nc2 >= 0 && nc * (nc + nc2) <= 2 * kFusedMaxCells * kFusedMaxCells;
+}
+
+// step sizes of one batched trial-step launch at most (one cluster each): the
+// clusters of a batch run side by side on the SMs that one cluster leaves idle
+constexpr int kTrialBatch = 16;
+
 template <class Real>
 struct DtTile {
     static constexpr int N = sizeof(Real) == 4 ? 2048 : 1024;   // records per shared-memory tile
@@ -101,7 +110,7 @@ __global__ void __launch_bounds__(kFusedThreads)
     dt_value_fused_kernel(int ncorner, int norm, const double* __restrict__ v, long long nv,
                           const int64_t* __restrict__ cells, long long nc, const double* __restrict__ c2,
                           const double* __restrict__ s2, long long nc2, double eps1, double eps2, double scale,
-                          FusedCoef cf, FusedShape fs, double* epart, double* energy) {
+                          FusedCoef cf, FusedShape fs, double* epart, double* energy, long long vstride) {
     constexpr int TILE = DtTile<Real>::N;
     extern __shared__ __align__(32) unsigned char fused_smem[];
     FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
@@ -112,6 +121,11 @@ __global__ void __launch_bounds__(kFusedThreads)
     const int local = tid % fs.tpt, g = tid / fs.tpt;
     const long long k = (long long)rank * fs.nc + local;
     const bool owner = local < fs.nc && k < nc;
+    // batched values: cluster b evaluates the vertex set v + b vstride into energy[b]
+    const long long b = blockIdx.x / fs.C;
+    v += b * vstride;
+    energy += b;
+    epart += b * kFusedMaxCluster;
     Real pk[5];
     for (int j = 0; j < 5; ++j) pk[j] = (Real)cf.pk[j];
     const long long total = nc + nc2;

@@ -46,6 +46,9 @@ struct DataArgs {
     const int64_t* vptr;
     const int64_t* vidx;
     double* px;
+    // batched values: vertex sets v + b vstride (b < nbatch) into energy[b]
+    int nbatch = 1;
+    long long vstride = 0;
 };
 
 // SYM (values): the cell-cell self part is evaluated once per unordered pair
@@ -166,26 +169,42 @@ int dt_impl(const DataArgs& a, Workspace& ws, cudaStream_t st) {
 template <class Real, int KIND, int PDEG, int D>
 int dt_value_fused(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     const FusedShape fs = fused_shape(a.nc);
-    double* epart = ws.take<double>(kFusedMaxCluster);
+    double* epart = ws.take<double>((size_t)kFusedMaxCluster * a.nbatch);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     FusedCoef cf{};
     for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
     for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
-    return launch_fused(dt_value_fused_kernel<Real, KIND, PDEG, D>, fs, dt_fused_smem<Real>(), dt_fused_smem<Real>(),
-                        st, a.ncorner, a.norm, a.v, (long long)a.nv, a.cells, (long long)a.nc, a.c2, a.s2,
-                        (long long)a.nc2, a.eps1, a.eps2, ks.scale, cf, fs, epart, a.energy);
+    return launch_fused(dt_value_fused_kernel<Real, KIND, PDEG, D>, fs, a.nbatch, dt_fused_smem<Real>(),
+                        dt_fused_smem<Real>(), st, a.ncorner, a.norm, a.v, (long long)a.nv, a.cells,
+                        (long long)a.nc, a.c2, a.s2, (long long)a.nc2, a.eps1, a.eps2, ks.scale, cf, fs, epart,
+                        a.energy, a.vstride);
 }
 
 template <class Real>
 int dt_run(const DataArgs& a, Workspace& ws, cudaStream_t st) {
+    const bool fused = a.px == nullptr && a.energy != nullptr && dt_fused_fits(a.nc, a.nc2);
+    if (a.nbatch > 1 && !fused) {
+        // general path: the vertex sets one after the other, each on the same workspace
+        const size_t off0 = ws.off;
+        size_t top = off0;
+        for (int b = 0; b < a.nbatch; ++b) {
+            DataArgs q = a;
+            q.nbatch = 1;
+            q.v = a.v ? a.v + (long long)b * a.vstride : nullptr;
+            q.energy = a.energy ? a.energy + b : nullptr;
+            ws.off = off0;
+            LDDMM_TRY(dt_run<Real>(q, ws, st));
+            top = std::max(top, ws.off);
+        }
+        ws.off = top;
+        return LDDMM_OK;
+    }
     auto go = [&](auto kind, auto pdeg, auto qdeg) {
         return dispatch_d(a.d, [&](auto D) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(pdeg)::value, Q_ = decltype(qdeg)::value,
                           D_ = decltype(D)::value;
-            if (a.px == nullptr && a.energy != nullptr && a.nc <= kFusedMaxCells &&
-                a.nc * (a.nc + a.nc2) <= 2 * kFusedMaxCells * kFusedMaxCells && a.d == D_)
-                return dt_value_fused<Real, K_, P_, D_>(a, ws, st);
+            if (fused && a.d == D_) return dt_value_fused<Real, K_, P_, D_>(a, ws, st);
             if (a.nc <= kSmallTargets) return dt_impl<Real, K_, P_, Q_, D_, true>(a, ws, st);
             return dt_impl<Real, K_, P_, Q_, D_>(a, ws, st);
         });
@@ -201,6 +220,11 @@ int dt_run(const DataArgs& a, Workspace& ws, cudaStream_t st) {
 }
 
 static int dt_validate(const DataArgs& a) {
+    if (a.nbatch < 1 || a.nbatch > (1 << 12) || (a.nbatch > 1 && (a.px != nullptr || a.vstride < a.nv * a.d))) {
+        set_error("dataterm: a batch needs 1 <= nbatch <= 4096, values only and vertex_stride >= nv * d "
+                  "(nbatch=%d vertex_stride=%lld)", a.nbatch, a.vstride);
+        return LDDMM_ERR_ARG;
+    }
     if ((a.ncorner != 2 && a.ncorner != 3) || a.norm < 0 || a.norm > 2 || a.nv < 1 || a.nc < 1 || a.nc2 < 0 ||
         a.d < 2 || a.d > 3 || !(a.sigma > 0) || a.order < 0 || a.eps1 < 0 || a.eps2 < 0 ||
         a.nv > (1LL << 30) || a.nc > (1LL << 30) || a.nc2 > (1LL << 30)) {
@@ -241,8 +265,11 @@ static int dt_validate(const DataArgs& a) {
 
 template <class Real>
 size_t dt_ws(int ncorner, int norm, int64_t nv, int d, int64_t nc, int64_t nc2, int order, int want_energy,
-             int want_grad) {
+             int want_grad, int nbatch = 1) {
+    if (nbatch < 1 || nbatch > (1 << 12) || (nbatch > 1 && (want_grad || !want_energy))) return 0;
     DataArgs a{};
+    a.nbatch = nbatch;
+    a.vstride = nv * d;
     a.ncorner = ncorner;
     a.norm = norm;
     a.nv = nv;
@@ -310,6 +337,39 @@ int lddmm_dataterm_f64(int cell_size, int norm, const double* vertices, int64_t 
                        const int64_t* vertex_idx, double* px, void* workspace, size_t workspace_bytes,
                        lddmm_stream_t stream) {
     DT_ARGS;
+    return dt_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+size_t lddmm_dataterm_value_batch_f32c_workspace(int cell_size, int norm, int64_t nv, int d, int64_t nc, int64_t nc2,
+                                                 int order, int nbatch) {
+    return dt_ws<float>(cell_size, norm, nv, d, nc, nc2, order, 1, 0, nbatch);
+}
+size_t lddmm_dataterm_value_batch_f64_workspace(int cell_size, int norm, int64_t nv, int d, int64_t nc, int64_t nc2,
+                                                int order, int nbatch) {
+    return dt_ws<double>(cell_size, norm, nv, d, nc, nc2, order, 1, 0, nbatch);
+}
+
+#define DT_BATCH_ARGS                                                                                           \
+    DataArgs a{cell_size, norm,  vertices, nv,   d,      cells,   nc,     tgt_centers, tgt_vectors, nc2, \
+               sigma,     order, eps1,     eps2, energy, nullptr, nullptr, nullptr};                      \
+    a.nbatch = nbatch;                                                                                  \
+    a.vstride = vertex_stride
+
+int lddmm_dataterm_value_batch_f32c(int cell_size, int norm, const double* vertices, int64_t nv, int d,
+                                    const int64_t* cells, int64_t nc, const double* tgt_centers,
+                                    const double* tgt_vectors, int64_t nc2, double sigma, int order, double eps1,
+                                    double eps2, int nbatch, int64_t vertex_stride, double* energy, void* workspace,
+                                    size_t workspace_bytes, lddmm_stream_t stream) {
+    DT_BATCH_ARGS;
+    return dt_entry<float>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int lddmm_dataterm_value_batch_f64(int cell_size, int norm, const double* vertices, int64_t nv, int d,
+                                   const int64_t* cells, int64_t nc, const double* tgt_centers,
+                                   const double* tgt_vectors, int64_t nc2, double sigma, int order, double eps1,
+                                   double eps2, int nbatch, int64_t vertex_stride, double* energy, void* workspace,
+                                   size_t workspace_bytes, lddmm_stream_t stream) {
+    DT_BATCH_ARGS;
     return dt_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

@@ -258,12 +258,18 @@ __global__ void __launch_bounds__(kFusedThreads) shoot_fused_kernel(const double
     const long long k = (long long)rank * fs.nc + local;
     const bool owner = local < fs.nc && k < n;
     const long long j0 = g * n / fs.S, j1 = (g + 1) * n / fs.S;
+    const long long N = n * D;
+    // batched trial steps: cluster b shoots at - eps[b] dir into slot b of the outputs
+    const long long b = blockIdx.x / fs.C;
+    xt += b * (T + 1) * N;
+    epart += b * kFusedMaxCluster;
+    if (energy != nullptr) energy += b;
+    if (at_try != nullptr) at_try += b * T * N;
     Real pk[5];
     for (int j = 0; j < 5; ++j) pk[j] = (Real)cf.pk[j];
     double c[3];
     fused_bbox_center(x0, n, D, scratch, c);
-    const long long N = n * D;
-    const double eps = dir != nullptr ? *epsp : 0.0;
+    const double eps = dir != nullptr ? epsp[b] : 0.0;
     for (long long i = tid; i < n; i += kFusedThreads) {
         double a0[3];
         for (int j = 0; j < D; ++j) a0[j] = shot_momentum(at, dir, eps, i * D + j);
@@ -488,10 +494,12 @@ inline size_t fused_dyn_smem(long long n, int D) {
            sizeof(double) * 6 * kFusedThreads;
 }
 
-// Launches `kernel` on one cluster of fs.C CTAs with `smem` bytes of dynamic
-// shared memory (`max_smem`: the kernel's opt-in limit, at least smem).
+// Launches `kernel` on `nbatch` clusters of fs.C CTAs (cluster b works on
+// problem b of a batch) with `smem` bytes of dynamic shared memory
+// (`max_smem`: the kernel's opt-in limit, at least smem).
 template <class Kern, class... Args>
-int launch_fused(Kern kernel, const FusedShape& fs, size_t smem, size_t max_smem, cudaStream_t st, Args... args) {
+int launch_fused(Kern kernel, const FusedShape& fs, int nbatch, size_t smem, size_t max_smem, cudaStream_t st,
+                 Args... args) {
     // the shared-memory opt-in, once per (device, kernel)
     static std::mutex mu;
     static std::set<std::pair<int, const void*>> done;
@@ -508,7 +516,7 @@ int launch_fused(Kern kernel, const FusedShape& fs, size_t smem, size_t max_smem
         }
     }
     cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(fs.C, 1, 1);
+    cfg.gridDim = dim3(fs.C * nbatch, 1, 1);
     cfg.blockDim = dim3(kFusedThreads, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;

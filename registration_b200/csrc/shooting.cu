@@ -19,6 +19,7 @@
 // adjoint) update in FP64, writes the packed planes of the next step and the
 // step's energy partials (one per combine block; the grid size depends only on
 // n, so the reduction order is fixed).
+#include "dataterm_fused.cuh"
 #include "fused_small.cuh"
 #include "host.h"
 #include "ops2.cuh"
@@ -28,6 +29,7 @@
 namespace lddmm {
 
 constexpr int kCombineThreads = 256;
+constexpr int kMaxBatch = 1 << 12;   // trial step sizes per batched call
 
 inline int combine_blocks(long long n) { return (int)std::min<long long>(1024, (n + kCombineThreads - 1) / kCombineThreads); }
 
@@ -190,6 +192,8 @@ struct ShootArgs {
     const double* dir = nullptr;
     const double* eps = nullptr;
     double* at_try = nullptr;
+    // batched trial steps: nbatch step sizes eps[0..nbatch), outputs at_try, xt, energy stacked per candidate
+    int nbatch = 1;
 };
 
 // at_try = at - (*eps) dir, rounded as two FP64 operations (the trial step of a line search)
@@ -243,14 +247,14 @@ int shoot_impl(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
 template <class Real, int KIND, int DEG, int D>
 int shoot_fused(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
     const FusedShape fs = fused_shape(a.n);
-    double* epart = ws.take<double>(kFusedMaxCluster);
+    double* epart = ws.take<double>((size_t)kFusedMaxCluster * a.nbatch);
     if (ws.measuring()) return LDDMM_OK;
     const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
     FusedCoef cf{};
     for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
     for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
     const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
-    return launch_fused(shoot_fused_kernel<Real, KIND, DEG, D>, fs, fused_dyn_smem<Real>(a.n, D),
+    return launch_fused(shoot_fused_kernel<Real, KIND, DEG, D>, fs, a.nbatch, fused_dyn_smem<Real>(a.n, D),
                         fused_dyn_smem<Real>(kFusedMaxPoints, 3), st, a.x0, a.at,
                         (long long)a.n, a.T, dt, ks.scale, cf, a.rw, fs, a.xt, a.energy, epart, a.dir, a.eps,
                         a.at_try);
@@ -259,7 +263,27 @@ int shoot_fused(const ShootArgs& a, Workspace& ws, cudaStream_t st) {
 template <class Real>
 int shoot_run(const ShootArgs& a0, Workspace& ws, cudaStream_t st) {
     ShootArgs a = a0;
-    if (a.dir != nullptr && !(a.n <= kFusedMaxPoints && a.d >= 2)) {
+    const bool fused = a.n <= kFusedMaxPoints && a.d >= 2;
+    if (a.nbatch > 1 && !fused) {
+        // general path: the candidates one after the other, each on the same workspace
+        const long long N = a.n * a.d;
+        const size_t off0 = ws.off;
+        size_t top = off0;
+        for (int b = 0; b < a.nbatch; ++b) {
+            ShootArgs q = a;
+            q.nbatch = 1;
+            q.eps = a.eps ? a.eps + b : nullptr;
+            q.at_try = a.at_try ? a.at_try + (long long)b * a.T * N : nullptr;
+            q.xt = a.xt ? a.xt + (long long)b * (a.T + 1) * N : nullptr;
+            q.energy = a.energy ? a.energy + b : nullptr;
+            ws.off = off0;
+            LDDMM_TRY(shoot_run<Real>(q, ws, st));
+            top = std::max(top, ws.off);
+        }
+        ws.off = top;
+        return LDDMM_OK;
+    }
+    if (a.dir != nullptr && !fused) {
         // general path: form the trial momenta, then shoot them
         if (!ws.measuring()) {
             const long long cnt = (long long)a.T * a.n * a.d;
@@ -412,7 +436,7 @@ int cov_fused(const CovArgs& a, Workspace& ws, cudaStream_t st) {
     for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
     for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
     const double dt = a.dt > 0 ? a.dt : 1.0 / a.T;
-    return launch_fused(cov_fused_kernel<Real, KIND, QDEG, D>, fs, fused_dyn_smem<Real>(a.n, D),
+    return launch_fused(cov_fused_kernel<Real, KIND, QDEG, D>, fs, 1, fused_dyn_smem<Real>(a.n, D),
                         fused_dyn_smem<Real>(kFusedMaxPoints, 3), st, a.xt, a.at,
                         a.px1, (long long)a.n, a.T, dt, ks.scale, ks.dscale, cf, a.rw, fs, a.pxt, a.dat);
 }
@@ -614,14 +638,16 @@ int run_with_workspace(Run run, const Args& a, void* wsp, size_t wsb, cudaStream
 }
 
 template <class Real>
-size_t shoot_ws(int64_t n, int d, int T) {
+size_t shoot_ws(int64_t n, int d, int T, int nbatch = 1) {
     if (basic_validate(n, d, T, 1.0, 10, "shoot") != LDDMM_OK) return 0;
+    if (nbatch < 1 || nbatch > kMaxBatch) return 0;
     ShootArgs a{};
     a.n = n;
     a.d = d;
     a.T = T;
     a.sigma = 1.0;
     a.order = 10;
+    a.nbatch = nbatch;
     Workspace ws;
     size_t best = 0;
     for (int order : {10, 3}) {  // the Laplacian and Gaussian plans may differ
@@ -640,7 +666,11 @@ int shoot_entry(const ShootArgs& a, void* wsp, size_t wsb, cudaStream_t st) {
     LDDMM_TRY(check_device_ptr(a.at, "at"));
     LDDMM_TRY(check_device_ptr(a.xt, "xt"));
     if (a.energy) LDDMM_TRY(check_device_ptr(a.energy, "energy"));
-    if (a.dir != nullptr || a.eps != nullptr || a.at_try != nullptr) {
+    if (a.dir != nullptr || a.eps != nullptr || a.at_try != nullptr || a.nbatch != 1) {
+        if (a.nbatch < 1 || a.nbatch > kMaxBatch) {
+            set_error("shoot: nbatch must be in [1, %d] (got %d)", kMaxBatch, a.nbatch);
+            return LDDMM_ERR_ARG;
+        }
         LDDMM_TRY(check_device_ptr(a.dir, "dir"));
         LDDMM_TRY(check_device_ptr(a.eps, "eps"));
         LDDMM_TRY(check_device_ptr(a.at_try, "at_try"));
@@ -753,6 +783,43 @@ int lddmm_shoot_along_f64(const double* x0, int64_t n, int d, const double* at, 
     a.eps = eps;
     a.at_try = at_try;
     return shoot_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+size_t lddmm_shoot_along_batch_f32c_workspace(int64_t n, int d, int T, int nbatch) {
+    return shoot_ws<float>(n, d, T, nbatch);
+}
+size_t lddmm_shoot_along_batch_f64_workspace(int64_t n, int d, int T, int nbatch) {
+    return shoot_ws<double>(n, d, T, nbatch);
+}
+
+int lddmm_shoot_along_batch_f32c(const double* x0, int64_t n, int d, const double* at, const double* dir,
+                                 const double* eps, int nbatch, int T, double dt, double sigma, int order,
+                                 double regweight, double* at_try, double* xt, double* energy, void* workspace,
+                                 size_t workspace_bytes, lddmm_stream_t stream) {
+    ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
+    a.dir = dir;
+    a.eps = eps;
+    a.at_try = at_try;
+    a.nbatch = nbatch;
+    return shoot_entry<float>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int lddmm_shoot_along_batch_f64(const double* x0, int64_t n, int d, const double* at, const double* dir,
+                                const double* eps, int nbatch, int T, double dt, double sigma, int order,
+                                double regweight, double* at_try, double* xt, double* energy, void* workspace,
+                                size_t workspace_bytes, lddmm_stream_t stream) {
+    ShootArgs a{x0, n, d, at, T, dt, sigma, order, regweight, xt, energy};
+    a.dir = dir;
+    a.eps = eps;
+    a.at_try = at_try;
+    a.nbatch = nbatch;
+    return shoot_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int lddmm_trial_batch_size(int64_t n, int d, int64_t nc, int64_t nc2) {
+    if (n < 1 || d < 2 || d > 3 || n > kFusedMaxPoints || !dt_fused_fits(nc, nc2)) return 1;
+    const int clusters = device_info().sms / fused_shape(n).C;
+    return std::max(1, std::min(kTrialBatch, clusters));
 }
 
 size_t lddmm_covector_f32c_workspace(int64_t n, int d, int T) { return cov_ws<float>(n, d, T); }

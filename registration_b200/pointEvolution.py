@@ -80,6 +80,43 @@ def shoot_along(x0, at, dir_, eps, KparDiff, regweight=1.0, at_try=None, energy_
     return at_try, xt, energy
 
 
+def shoot_along_batch(x0, at, dir_, eps, KparDiff, regweight=1.0, at_try=None, xt=None, energy=None):
+    """Device call: the shots of at - eps[b] dir for every step size of the FP64
+    device vector eps (nbatch,); returns (at_try (nbatch, T, N, dim), xt
+    (nbatch, T+1, N, dim), energy (nbatch,)), slot b bit-identical to
+    shoot_along with eps[b].  Outputs given as arguments must be contiguous."""
+    require_cuda()
+    x0d, atd, dd = to_dev(x0), to_dev(at), to_dev(dir_)
+    T, n, d = atd.shape
+    if dd.shape != atd.shape or x0d.shape != (n, d):
+        raise ValueError("x0 must be (N, dim), at and dir (T, N, dim)")
+    if not (isinstance(eps, torch.Tensor) and eps.is_cuda and eps.dtype == torch.float64 and eps.dim() == 1
+            and eps.is_contiguous() and eps.numel() >= 1):
+        raise ValueError("eps must be a contiguous FP64 device vector of the step sizes")
+    B = eps.numel()
+    sigma, order, sfx = _kernel_args(KparDiff)
+    want = {"at_try": (B, T, n, d), "xt": (B, T + 1, n, d), "energy": (B,)}
+    outs = {"at_try": at_try, "xt": xt, "energy": energy}
+    for k, shape in want.items():
+        if outs[k] is None:
+            outs[k] = torch.empty(shape, dtype=torch.float64, device=x0d.device)
+        elif tuple(outs[k].shape) != shape or not outs[k].is_contiguous() or outs[k].dtype != torch.float64:
+            raise ValueError("%s must be a contiguous FP64 tensor of shape %s" % (k, shape))
+    wsb = _lib.query("lddmm_shoot_along_batch_%s_workspace" % sfx, n, d, T, B)
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_shoot_along_batch_" + sfx, ptr(x0d), n, d, ptr(atd), ptr(dd), ptr(eps), B, T, 0.0, sigma,
+              order, float(regweight), ptr(outs["at_try"]), ptr(outs["xt"]), ptr(outs["energy"]), ptr(ws), wsb,
+              stream_handle())
+    return outs["at_try"], outs["xt"], outs["energy"]
+
+
+def trial_batch_size(n, d, ncells, ncells_target):
+    """Step sizes that one batched trial launch evaluates side by side (1: the
+    problem is too large for the single-cluster kernels, batches would run one
+    step size after the other)."""
+    return max(1, _lib.query("lddmm_trial_batch_size", int(n), int(d), int(ncells), int(ncells_target)))
+
+
 def covector(xt, at, px1, KparDiff, regweight, with_dat=True, dt=None):
     """Device call: returns (pxt, dat) given the trajectory xt (T+1, N, dim); dt defaults to 1/T."""
     require_cuda()
