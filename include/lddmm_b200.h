@@ -196,6 +196,23 @@ LDDMM_API int lddmm_covector_f64(const double* xt, int64_t n, int d, const doubl
                                  const double* px1, double sigma, int order, double regweight, double* pxt,
                                  double* dat, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
+/* ---- metric inner products of directions: Matching.dotProduct -----------------
+ * Replaces the loops of py-lddmm/surfaceMatching.py:353-377 and
+ * curveMatching.py:286-304 (no affine part):
+ *   out[l] = sum_{t<T} sum_k <g2[l][t][k], sum_j K(xt[t][k], xt[t][j]) g1[t][j]>,  l < m <= 8
+ * xt (>= T, n, d) the trajectory (rows 0..T-1), g1 (T, n, d), g2: a HOST array of
+ * m device pointers to (T, n, d) arrays, out: m doubles on the device.  Kernel
+ * sums in FP32 with compensated partials (f32c) or FP64, dot products and all
+ * reductions in FP64 in a fixed order (two launches for all T steps). */
+LDDMM_API size_t lddmm_metric_dots_f32c_workspace(int64_t n, int d, int T, int m);
+LDDMM_API int lddmm_metric_dots_f32c(const double* xt, int64_t n, int d, int T, const double* g1,
+                                     const double* const* g2, int m, double sigma, int order, double* out,
+                                     void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+LDDMM_API size_t lddmm_metric_dots_f64_workspace(int64_t n, int d, int T, int m);
+LDDMM_API int lddmm_metric_dots_f64(const double* xt, int64_t n, int d, int T, const double* g1,
+                                    const double* const* g2, int m, double sigma, int order, double* out,
+                                    void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+
 /* ---- EPDiff shooting: pointEvolution.landmarkEPDiff ---------------------------
  * Replaces py-lddmm/pointEvolution.py:599-658 (no affine / optional outputs):
  *   xt[k+1] = xt[k] + dt K(xt[k]) at[k],

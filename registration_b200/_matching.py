@@ -74,6 +74,7 @@ class DeviceMatching:
         self.calls = {"updateTry": 0, "getGradient": 0, "dotProduct": 0}
         self.cudaGraphs = bool(cudaGraphs)
         self._graph = None
+        self._grad_graph = None
         self.obj = None
         self.objTry = None
         self.gradCoeff = self.npt
@@ -149,8 +150,11 @@ class DeviceMatching:
         return float(self._data_energy(to_dev(_fvDef.vertices)))
 
     def endPointGradient(self):
+        return self._end_point_gradient(self.xt[-1])
+
+    def _end_point_gradient(self, x_end):
         if self._fast_data:
-            _, px = _dt.dataterm(self.param.errorType, self.xt[-1], self._dshape, self._tc, self._tv,
+            _, px = _dt.dataterm(self.param.errorType, x_end, self._dshape, self._tc, self._tv,
                                  self.param.KparDist, energy=False, grad=True)
         else:
             px = to_dev(self.param.fun_objGrad(self.fvDef, self.fv1, self.param.KparDist))
@@ -315,12 +319,53 @@ class DeviceMatching:
     def getGradient(self, coeff=1.0):
         """(surfaceMatching.py:301-327): grd.diff = (2 rw a - p_{t+1}) / (coeff T)."""
         self.calls["getGradient"] += 1
-        px1 = -self.endPointGradient()
-        _, dat = evol.covector(self.xt, self.at, px1, self.param.KparDiff, self.regweight, with_dat=True)
         grd = Direction()
-        grd.diff = dat / (coeff * self.Tsize)
+        if (self.cudaGraphs and self._fast_data and self.npt <= 2048
+                and type(self).endPointGradient is DeviceMatching.endPointGradient):
+            grd.diff = self._graph_gradient(float(coeff))
+        else:
+            px1 = -self.endPointGradient()
+            _, dat = evol.covector(self.xt, self.at, px1, self.param.KparDiff, self.regweight, with_dat=True)
+            grd.diff = dat / (coeff * self.Tsize)
         grd.aff = np.zeros(self.Afft.shape)
         return grd
+
+    def _gradient_body(self, xt, at, coeff):
+        px1 = -self._end_point_gradient(xt[-1])
+        _, dat = evol.covector(xt, at, px1, self.param.KparDiff, self.regweight, with_dat=True)
+        return dat / (coeff * self.Tsize)
+
+    def _graph_gradient(self, coeff):
+        """The data-term gradient, the adjoint and the scaling replayed from a CUDA
+        graph (the same kernels on copies of xt and at: bit-identical to the
+        eager path); a small problem's dozen launches become one."""
+        g = self._grad_graph
+        if g is None or g["coeff"] != coeff:
+            import types
+            g = self._grad_graph = {"coeff": coeff, "xt": self.xt.clone(), "at": self.at.clone(),
+                                    "xt_src": self.xt, "at_src": self.at, "owner": types.SimpleNamespace()}
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(side):
+                with workspace.scope(g["owner"]):
+                    self._gradient_body(g["xt"], g["at"], coeff)
+                with workspace.scope(g["owner"]):
+                    graph.capture_begin()
+                    try:
+                        g["dat"] = self._gradient_body(g["xt"], g["at"], coeff)
+                    finally:
+                        graph.capture_end()
+            torch.cuda.current_stream().wait_stream(side)
+            g["graph"] = graph
+        if g["xt_src"] is not self.xt:
+            g["xt"].copy_(self.xt)
+            g["xt_src"] = self.xt
+        if g["at_src"] is not self.at:
+            g["at"].copy_(self.at)
+            g["at_src"] = self.at
+        g["graph"].replay()
+        return g["dat"].clone()
 
     def addProd(self, dir1, dir2, beta):
         d = Direction()
@@ -344,6 +389,9 @@ class DeviceMatching:
         """sum_t <g2_t, K(x_t) g1_t> (surfaceMatching.py:353-377), FP64 on the device."""
         self.calls["dotProduct"] += 1
         K = self.param.KparDiff
+        if K.precision == 'fp32c' and self.npt <= 2048 and 1 <= len(g2) <= 8:
+            # all T steps and directions in two launches (pointEvolution.metric_dots)
+            return evol.metric_dots(self.xt, g1.diff, [gr.diff for gr in g2], K).cpu().numpy()
         if K.precision == 'fp32c':
             # the T applyK sums as one ragged launch (one segment per time step)
             T, N, d = self.Tsize, self.npt, self.dim

@@ -14,6 +14,8 @@ arguments that the matching code passes for affine='none' are accepted.
 
 numpy in -> numpy out; CUDA tensors in -> CUDA tensors out.
 """
+import ctypes
+
 import numpy as np
 import torch
 
@@ -115,6 +117,30 @@ def trial_batch_size(n, d, ncells, ncells_target):
     problem is too large for the single-cluster kernels, batches would run one
     step size after the other)."""
     return max(1, _lib.query("lddmm_trial_batch_size", int(n), int(d), int(ncells), int(ncells_target)))
+
+
+def metric_dots(xt, g1, g2s, KparDiff):
+    """Device call: the FP64 device vector (len(g2s),) of
+    sum_t sum_k <g2[t][k], sum_j K(xt[t][k], xt[t][j]) g1[t][j]> over the T = len(g1)
+    steps of the trajectory xt (T+1 or T, N, dim), one entry per g2 in g2s (<= 8);
+    the metric inner products of Matching.dotProduct in two launches."""
+    require_cuda()
+    xtd, g1d = to_dev(xt), to_dev(g1)
+    g2d = [to_dev(g) for g in g2s]
+    T, n, d = g1d.shape
+    if xtd.shape[0] < T or tuple(xtd.shape[1:]) != (n, d) or any(tuple(g.shape) != (T, n, d) for g in g2d):
+        raise ValueError("xt must be (>= T, N, dim), g1 and every g2 (T, N, dim)")
+    if not 1 <= len(g2d) <= 8:
+        raise ValueError("1 to 8 directions g2")
+    sigma, order, sfx = _kernel_args(KparDiff)
+    out = torch.empty(len(g2d), dtype=torch.float64, device=xtd.device)
+    ptrs = (ctypes.c_void_p * len(g2d))(*[g.data_ptr() for g in g2d])
+    wsb = _lib.query("lddmm_metric_dots_%s_workspace" % sfx, n, d, T, len(g2d))
+    ws = workspace.get(wsb)
+    _lib.call("lddmm_metric_dots_" + sfx, ptr(xtd), n, d, T, ptr(g1d), ctypes.cast(ptrs, ctypes.c_void_p), len(g2d),
+              sigma, order, ptr(out),
+              ptr(ws), wsb, stream_handle())
+    return out
 
 
 def covector(xt, at, px1, KparDiff, regweight, with_dat=True, dt=None):
