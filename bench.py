@@ -351,10 +351,33 @@ def run_curve(args):
                "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}},
               dtype="f64")
         return 0
+    m = curve_measure(iters, sig_err, args.steps, args.warmup, not args.no_cpu_baseline)
+    config["statistic"] = "median of the timed steps (host-bound workload)"
+    _line(args, "curve matches/s", m["matches_per_s"], "matches/s", True, config,
+          {"ms_per_step": m["ms_per_match"], "ms_per_step_mean": m["ms_per_match_mean"], "step_ms": m["step_ms"],
+           "final_energy_fp32c": m["final_energy"], "final_energy_fp64": m["fp64_gpu"]["final_energy"],
+           "final_energy_abs_diff": abs(m["final_energy"] - m["fp64_gpu"]["final_energy"]),
+           "iterations": m["iterations"], "iterations_fp64": m["fp64_gpu"]["iterations"], "calls": m["calls"],
+           "fp64_gpu_ms": m["fp64_gpu"]["ms_per_match"],
+           "fp32c_with_auto_line_search": m["fp32c_with_auto_line_search"],
+           "cpu_baseline": m["cpu_baseline"],
+           "e2e": {"value": m["matches_per_s"], "unit": "matches/s", "h2d_bytes_per_step": m["h2d_bytes"],
+                   "d2h_bytes_per_step": m["d2h_bytes"]}})
+    return 0
+
+
+def curve_measure(iters, sig_err, steps, warmup, with_cpu):
+    """The 256-vertex curve match: FP32c kernel sums and FP64 reductions with
+    FP64 data-term values in the line search (at 256 cells an FP64 value costs
+    about what an FP32c one does, and the FP32c difference errors of this curve
+    exceed the 'auto' bound's floor), timed `steps` times after `warmup`
+    matches; beside it the 'auto' line search, the plain FP64 path and, with
+    with_cpu, one match of the FP64 oracle on the host cores."""
     import torch
     from registration_b200 import curveMatching as CM
     from registration_b200 import curves as cv
     from registration_b200 import kernelFunctions as kf
+    v, vt = curve_problem()
 
     def match(precision, lsp=None):
         param = CM.CurveMatchingParam(timeStep=0.1, KparDiff=kf.Kernel(name="gauss", sigma=0.5, precision=precision),
@@ -369,20 +392,16 @@ def run_curve(args):
         torch.cuda.synchronize()
         return time.perf_counter() - t0, cm
 
-    # headline: FP32c kernel sums and FP64 reductions with FP64 data-term values
-    # in the line search (at 256 cells an FP64 value costs about what an FP32c
-    # one does, and the FP32c difference errors of this curve exceed the 'auto'
-    # bound's floor); beside it the 'auto' line search and the plain FP64 path
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         match("fp32c", "fp64")
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         dt_, cm = match("fp32c", "fp64")
         times.append(dt_)
-    t_ls64, cm_ls64 = match("fp32c", "auto")
+    t_ls, cm_ls = match("fp32c", "auto")
     t64, cm64 = match("fp64")
     cpu = None
-    if not args.no_cpu_baseline:
+    if with_cpu:
         import oracle
         from oracle import lddmm_ref as ref
         oracle.build()
@@ -396,22 +415,22 @@ def run_curve(args):
         tc = time.perf_counter() - t0
         cpu = {"value": 1.0 / tc, "unit": "matches/s", "cores": os.cpu_count(), "kind": "port",
                "sample": "one whole match (FP64 numpy + C/OpenMP loops)", "final_energy": rcm.obj}
-    # a 256-point match is ~50k short launches driven from Python: host-bound and
-    # sensitive to load on the (shared) host, so the median step is the value
-    val = 1.0 / float(np.median(times))
-    config["statistic"] = "median of the timed steps (host-bound workload)"
-    _line(args, "curve matches/s", val, "matches/s", True, config,
-          {"ms_per_step": 1e3 * float(np.median(times)), "ms_per_step_mean": 1e3 * float(np.mean(times)),
-           "step_ms": [round(1e3 * t, 2) for t in times],
-           "final_energy_fp32c": cm.obj, "final_energy_fp64": cm64.obj,
-           "final_energy_abs_diff": abs(cm.obj - cm64.obj), "iterations": cm.iter, "iterations_fp64": cm64.iter,
-           "calls": cm.calls, "fp64_gpu_ms": 1e3 * t64,
-           "fp32c_with_auto_line_search": {"ms": 1e3 * t_ls64, "final_energy": cm_ls64.obj,
-                                           "iterations": cm_ls64.iter},
-           "cpu_baseline": cpu,
-           "e2e": {"value": val, "unit": "matches/s", "h2d_bytes_per_step": int(v.nbytes + vt.nbytes),
-                   "d2h_bytes_per_step": int(cm.at.numel() * 8)}})
-    return 0
+    # a match is about 1,300 short launches and 300 host read-backs driven from
+    # Python: host-bound and sensitive to load on the (shared) host, so the
+    # median step is the value
+    med = float(np.median(times))
+    return {"workload": "curve matching: ellipse 256 vertices, 4 bumps, gauss sigma 0.5, current sigma 0.5, "
+                        "sigmaError %g, T 10, at most %d cg iterations" % (sig_err, iters),
+            "matches_per_s": 1.0 / med, "ms_per_match": 1e3 * med, "ms_per_match_mean": 1e3 * float(np.mean(times)),
+            "step_ms": [round(1e3 * t, 2) for t in times], "statistic": "median of the timed matches",
+            "line_search": "fp64 values", "final_energy": float(cm.obj), "iterations": cm.iter,
+            "calls": dict(cm.calls),
+            "fp32c_with_auto_line_search": {"ms": 1e3 * t_ls, "final_energy": float(cm_ls.obj),
+                                            "iterations": cm_ls.iter},
+            "fp64_gpu": {"ms_per_match": 1e3 * t64, "matches_per_s": 1.0 / t64, "final_energy": float(cm64.obj),
+                         "iterations": cm64.iter},
+            "cpu_baseline": cpu,
+            "h2d_bytes": int(v.nbytes + vt.nbytes), "d2h_bytes": int(cm.at.numel() * 8)}
 
 
 def surface_measure(iters, sig_err, steps, with_ls64=True):
@@ -470,14 +489,17 @@ def surface_summary(m, sig_err, iters):
 
 
 def matching_records(args):
-    """The metric's matching clause beside the kernel-sum line: the surface
-    workload (sigmaError 0.01, at most 100 cg iterations; 'auto' line search
-    and the plain FP64 GPU path) and a short served stream of
+    """The metric's matching clause beside the kernel-sum line: the 256-vertex
+    curve match (sigmaError 0.02, at most 50 cg iterations, with one FP64
+    oracle match on the host cores), the surface workload (sigmaError 0.01, at
+    most 100 cg iterations; 'auto' line search and the plain FP64 GPU path) and
+    a short served stream of
     --serve-requests requests (sigmaError 0.01, at most 50 iterations each)
     with both one-at-a-time baselines measured on every request."""
     import logging
     logging.disable(logging.INFO)
     try:
+        curve = curve_measure(50, 0.02, steps=10, warmup=2, with_cpu=True)
         sig_err, iters = 0.01, 100
         surf = surface_summary(surface_measure(iters, sig_err, steps=1, with_ls64=False), sig_err, iters)
         served = None
@@ -487,7 +509,7 @@ def matching_records(args):
             served = serving_summary(m, args.serve_requests, 50, sig_err, ekw)
     finally:
         logging.disable(logging.NOTSET)
-    return surf, served
+    return curve, surf, served
 
 
 def run_surface(args):
@@ -1221,7 +1243,7 @@ def main():
         }
         if world == 1 and not args.no_matching:
             del flush
-            line["surface_matching"], line["served_matching"] = matching_records(args)
+            line["curve_matching"], line["surface_matching"], line["served_matching"] = matching_records(args)
         print(json.dumps(line), flush=True)
     workspace.clear()
     if world > 1:

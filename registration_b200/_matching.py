@@ -46,6 +46,39 @@ class Direction:
 class DeviceMatching:
     """Subclasses set: fv0, fv1 (shapes), param, norm_name, tgt_vectors_attr."""
 
+    # The best trial step's momenta and trajectory.  A batched trial leaves them
+    # in a slot of the batch buffers; they are copied out only when read, when
+    # accepted, or before the next batch overwrites the slot.
+    _pending_try = None
+
+    def _materialize_try(self):
+        pend = self._pending_try
+        if pend is not None:
+            g, b = pend
+            self._pending_try = None
+            self.__dict__["_atTry"] = g["atTry"][b].clone()
+            self.__dict__["_xtTry"] = g["xt"][b].clone()
+
+    @property
+    def atTry(self):
+        self._materialize_try()
+        return self.__dict__.get("_atTry")
+
+    @atTry.setter
+    def atTry(self, v):
+        self._materialize_try()
+        self.__dict__["_atTry"] = v
+
+    @property
+    def xtTry(self):
+        self._materialize_try()
+        return self.__dict__.get("_xtTry")
+
+    @xtTry.setter
+    def xtTry(self, v):
+        self._materialize_try()
+        self.__dict__["_xtTry"] = v
+
     def _init_state(self, maxIter, regWeight, verb, testGradient, affine, symmetric, lineSearchPrecision='fp64',
                     noise=1e-8, cudaGraphs=True):
         require_cuda()
@@ -292,6 +325,7 @@ class DeviceMatching:
         cache = g["cache"]
         eps = float(eps)
         if eps not in cache:
+            self._materialize_try()     # the slots are about to be overwritten
             ladder = self._trial_ladder(eps, cache, dir.diff)
             g["eps_host"].numpy()[:] = ladder
             g["eps"].copy_(g["eps_host"], non_blocking=True)
@@ -311,9 +345,8 @@ class DeviceMatching:
             logging.info('Warning: nan in updateTry')
             return 1e500
         if (objRef is None) or (objTry < objRef):
-            self.atTry = g["atTry"][b].clone()
+            self._pending_try = (g, b)
             self.objTry = objTry
-            self.xtTry = g["xt"][b].clone()
         return objTry
 
     def getGradient(self, coeff=1.0):
@@ -408,6 +441,16 @@ class DeviceMatching:
 
     def acceptVarTry(self):
         self.obj = self.objTry
+        pend = self._pending_try
+        if pend is not None:
+            # one copy out of the batch slot (the eager path's atTry.clone())
+            g, b = pend
+            self._pending_try = None
+            self.at = g["atTry"][b].clone()
+            self.xt = g["xt"][b].clone()
+            self.__dict__["_atTry"] = self.at
+            self.__dict__["_xtTry"] = self.xt
+            return
         self.at = self.atTry.clone()
         if self.xtTry is not None:
             self.xt = self.xtTry

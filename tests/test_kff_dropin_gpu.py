@@ -88,8 +88,13 @@ def _oracle_routed_through(kff, monkeypatch):
         monkeypatch.setattr(oracle, nm, fn)
 
 
-def _check_stack(kff, make, want, at_final, precision):
-    """fp64: the whole trace; fp32c: objective and gradient at the final momenta."""
+def _check_stack(kff, make, want, at_final, precision, make_far=None):
+    """fp64: the whole trace; fp32c: the objective at the final momenta and the
+    gradient at zero momenta.  The gradient there is the data-term gradient
+    d(<S1,S1> - 2 <S1,S2>), a difference of sums whose FP32c error is relative
+    to the sums: the bar is 1e-5 of the self term's gradient d<S1,S1>, the
+    gradient of the same problem with the target moved out of reach of the
+    kernel (make_far)."""
     if precision == "fp64":
         m = make()
         trace = []
@@ -108,14 +113,15 @@ def _check_stack(kff, make, want, at_final, precision):
     # gradient (K s1 - K s2) and the momentum gradient (2 rw a - p) are small
     # differences of large sums, whose FP32c error is relative to the sums
     grads = {}
-    for prec in ("fp64", "fp32c"):
-        kff.set_precision(prec)
-        m = make()
+    for prec, mk in (("fp64", make), ("fp32c", make), ("self", make_far)):
+        kff.set_precision("fp64" if prec == "self" else prec)
+        m = mk()
         m.obj = None
         m.objectiveFun()
         grads[prec] = m.getGradient(m.gradCoeff).diff
-    g32, g64 = grads["fp32c"], grads["fp64"]
-    assert np.linalg.norm(g32 - g64) <= 1e-5 * np.linalg.norm(g64)
+    g32, g64, gself = grads["fp32c"], grads["fp64"], grads["self"]
+    assert np.linalg.norm(g32 - g64) <= 1e-5 * np.linalg.norm(gself), (
+        np.linalg.norm(g32 - g64), np.linalg.norm(g64), np.linalg.norm(gself))
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
@@ -128,7 +134,8 @@ def test_matching_stack_on_the_dropin_reproduces_reference_traces(kff, golden, m
     param = ref.MatchingParam(timeStep=0.2, KparDiff=ref.Kernel(name="gauss", sigma=0.4),
                               KparDist=ref.Kernel(name="gauss", sigma=0.3), sigmaError=0.5, errorType=err)
     make = lambda: ref.SurfaceMatching(ref.Surface(FV=[f, v0]), ref.Surface(FV=[f, v1]), param, maxIter=6)
-    _check_stack(kff, make, golden["sm_%s_trace" % err], golden["sm_%s_at" % err], precision)
+    far = lambda: ref.SurfaceMatching(ref.Surface(FV=[f, v0]), ref.Surface(FV=[f, v1 + 1e3]), param, maxIter=6)
+    _check_stack(kff, make, golden["sm_%s_trace" % err], golden["sm_%s_at" % err], precision, far)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
@@ -141,7 +148,9 @@ def test_curve_matching_on_the_dropin_reproduces_reference_trace(kff, golden, mo
                               curves=True)
     make = lambda: ref.CurveMatching(ref.Curve(pointSet=golden["cm_v0"]), ref.Curve(pointSet=golden["cm_v1"]),
                                      param, maxIter=8)
-    _check_stack(kff, make, golden["cm_current_trace"], golden["cm_current_at"], precision)
+    far = lambda: ref.CurveMatching(ref.Curve(pointSet=golden["cm_v0"]), ref.Curve(pointSet=golden["cm_v1"] + 1e3),
+                                    param, maxIter=8)
+    _check_stack(kff, make, golden["cm_current_trace"], golden["cm_current_at"], precision, far)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
