@@ -172,10 +172,12 @@ LDDMM_API int lddmm_shoot_along_batch_f64(const double* x0, int64_t n, int d, co
                                           void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* How many trial steps of a problem (n points in d dimensions, a data term of
- * nc own and nc2 target cells) one batched launch runs side by side: 1 when the
- * batch would run one step size after the other (the general path), else up
- * to 16, bounded by the SMs over the cluster size. */
-LDDMM_API int lddmm_trial_batch_size(int64_t n, int d, int64_t nc, int64_t nc2);
+ * nc own and nc2 target cells; shot and value kernel sums in FP64 when
+ * shot_fp64 / value_fp64, else FP32c) one batched launch runs side by side:
+ * 1 when the batch would run one step size after the other (the general
+ * path), else up to 24, bounded by the clusters of the shot and value kernels
+ * that are resident on the device at once. */
+LDDMM_API int lddmm_trial_batch_size(int64_t n, int d, int64_t nc, int64_t nc2, int shot_fp64, int value_fp64);
 
 /* ---- Hamiltonian adjoint: landmarkHamiltonianCovector / Gradient --------------
  * Replaces the backward loop of py-lddmm/pointEvolution.py:735-765 and the

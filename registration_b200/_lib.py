@@ -48,7 +48,7 @@ SIGNATURES = {
                                           _P]),
     "lddmm_shoot_along_batch_f64": (_I, [_P, _I64, _I, _P, _P, _P, _I, _I, _D, _D, _I, _D, _P, _P, _P, _P, _SZ,
                                          _P]),
-    "lddmm_trial_batch_size": (_I, [_I64, _I, _I64, _I64]),
+    "lddmm_trial_batch_size": (_I, [_I64, _I, _I64, _I64, _I, _I]),
     "lddmm_metric_dots_f32c_workspace": (_SZ, [_I64, _I, _I, _I]),
     "lddmm_metric_dots_f64_workspace": (_SZ, [_I64, _I, _I, _I]),
     "lddmm_metric_dots_f32c": (_I, [_P, _I64, _I, _I, _P, _P, _I, _D, _I, _P, _P, _SZ, _P]),

@@ -24,6 +24,8 @@ runs the adjoint on that stored trajectory instead of re-shooting inside
 landmarkHamiltonianGradient (the shots are deterministic, so they would be
 bit-identical).
 """
+import contextlib
+import gc
 import logging
 
 import numpy as np
@@ -34,6 +36,20 @@ from . import _ragged as _rg
 from . import pointEvolution as evol
 from ._precision import _Value, value_bound
 from .device import require_cuda, to_dev, workspace
+
+
+@contextlib.contextmanager
+def _gc_paused():
+    """Python's cycle collector paused while a CUDA graph is captured: a
+    collection that falls inside the capture costs milliseconds and frees
+    nothing the capture needs."""
+    was = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if was:
+            gc.enable()
 
 
 class Direction:
@@ -258,24 +274,50 @@ class DeviceMatching:
         (cg's tiny-step probe).  Changes no value, only what a batch holds."""
         self._hint = (dir.diff, [float(e) for e in steps])
 
+    # halving steps of a batch, and the halving depths (counted from the first
+    # trial of an iteration) whose growth steps it also holds: cg restarts each
+    # iteration at 100 times the last accepted step, so the search returns to
+    # that scale after about log2(100) ~ 7 halvings and grows from there
+    _LADDER_HALVINGS = 12
+    _LADDER_GROWTH_DEPTHS = (5, 6, 7, 8, 9, 10, 11, 4)
+
     def _trial_ladder(self, eps, cache, dir_diff):
-        """The step sizes to evaluate with `eps`: the ones cg tries next from it
-        (conjugateGradient.py:140-183), computed with cg's own operations so
-        that they compare equal: eps 1.25^j (chained) when eps is a growth step
-        of an evaluated size, else eps / 2^k (the halving loops) and the hinted
-        steps of this direction."""
+        """The step sizes to evaluate with `eps`: the ones cg may try next from
+        it (conjugateGradient.py:140-183), computed with cg's own operations so
+        that they compare equal.  When eps is a growth step of an evaluated
+        size: eps 1.25^j (chained).  Otherwise eps / 2^k (the halving loops),
+        the hinted steps of this direction (cg's tiny-step probe), then the
+        first growth steps 1.25 h, 1.25 (1.25 h) of the likely accepted
+        halvings h, while the batch has room."""
         B = self._graph["B"]
         if B == 1:
             return [eps]
+        if any(1.25 * e == eps for e in cache):
+            ladder = [eps]
+            while len(ladder) < B:
+                ladder.append(1.25 * ladder[-1])
+            return ladder
         hint = getattr(self, "_hint", None)
         extra = [e for e in hint[1] if e != eps] if hint is not None and hint[0] is dir_diff else []
-        grow = any(1.25 * e == eps for e in cache)
-        if grow:
-            extra = []
-        ladder = [eps]
-        while len(ladder) < B - len(extra):
-            ladder.append(1.25 * ladder[-1] if grow else ladder[-1] / 2)
-        return ladder + [e for e in extra if e not in ladder][:B - len(ladder)]
+        halving = [eps]
+        while len(halving) < min(self._LADDER_HALVINGS, B - len(extra)):
+            halving.append(halving[-1] / 2)
+        ladder = halving + [e for e in extra if e not in halving]
+        depth = 1 if B < 24 else 2
+        for k in self._LADDER_GROWTH_DEPTHS:
+            if k >= len(halving):
+                continue
+            g = halving[k]
+            for _ in range(depth):
+                g = 1.25 * g
+                if len(ladder) < B and g not in ladder:
+                    ladder.append(g)
+        h = halving[-1]
+        while len(ladder) < B:     # deeper halvings fill what is left
+            h = h / 2
+            if h not in ladder:
+                ladder.append(h)
+        return ladder[:B]
 
     def _graph_update_try(self, dir, eps, objRef):
         """updateTry with the trial steps replayed from a CUDA graph captured on
@@ -288,7 +330,8 @@ class DeviceMatching:
         g = self._graph
         if g is None:
             dev = self.x0.device
-            B = evol.trial_batch_size(self.npt, self.dim, self._dshape.cells.shape[0], self._tc.shape[0])
+            B = evol.trial_batch_size(self.npt, self.dim, self._dshape.cells.shape[0], self._tc.shape[0],
+                                      self.param.KparDiff.precision, self._Kval.precision)
             T, n, d = self.at.shape
             g = self._graph = {"B": B, "at": self.at.clone(), "dir": dir.diff.clone(),
                                "eps": torch.full((B,), float(eps), dtype=torch.float64, device=dev),
@@ -303,7 +346,7 @@ class DeviceMatching:
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.stream(side):
+            with _gc_paused(), torch.cuda.stream(side):
                 with workspace.scope(self):
                     self._trial_body()      # sizes the private workspaces, initialises lazily created state
                 with workspace.scope(self):
@@ -380,7 +423,7 @@ class DeviceMatching:
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.stream(side):
+            with _gc_paused(), torch.cuda.stream(side):
                 with workspace.scope(g["owner"]):
                     self._gradient_body(g["xt"], g["at"], coeff)
                 with workspace.scope(g["owner"]):

@@ -42,7 +42,12 @@ inline bool dt_fused_fits(long long nc, long long nc2) {
 
 // step sizes of one batched trial-step launch at most (one cluster each): the
 // clusters of a batch run side by side on the SMs that one cluster leaves idle
-constexpr int kTrialBatch = 16;
+// (at 256 points, 24 clusters of 8 CTAs take the time of one)
+constexpr int kTrialBatch = 24;
+
+// clusters of the single-launch value kernel (Gaussian instance) for nc own and
+// nc2 target cells that are resident at once (defined with the kernel's launches)
+int dt_value_resident_clusters(long long nc, long long nc2, int d, int fp64);
 
 template <class Real>
 struct DtTile {
@@ -110,11 +115,11 @@ __global__ void __launch_bounds__(kFusedThreads)
     dt_value_fused_kernel(int ncorner, int norm, const double* __restrict__ v, long long nv,
                           const int64_t* __restrict__ cells, long long nc, const double* __restrict__ c2,
                           const double* __restrict__ s2, long long nc2, double eps1, double eps2, double scale,
-                          FusedCoef cf, FusedShape fs, double* epart, double* energy, long long vstride) {
-    constexpr int TILE = DtTile<Real>::N;
+                          FusedCoef cf, FusedShape fs, double* epart, double* energy, long long vstride,
+                          int tile) {
     extern __shared__ __align__(32) unsigned char fused_smem[];
     FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
-    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * TILE);
+    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * tile);
     double* scratch = red + kFusedThreads;
     const int rank = (int)cluster_rank();
     const int tid = threadIdx.x;
@@ -183,8 +188,8 @@ __global__ void __launch_bounds__(kFusedThreads)
     FusedAcc<Real, 1> acc;
     acc.zero();
     constexpr int FOLD = sizeof(Real) == 4 ? 32 : 1 << 30;
-    for (long long t0 = 0; t0 < total; t0 += TILE) {
-        const int len = (int)(total - t0 < TILE ? total - t0 : TILE);
+    for (long long t0 = 0; t0 < total; t0 += tile) {
+        const int len = (int)(total - t0 < tile ? total - t0 : tile);
         for (int i = tid; i < len; i += kFusedThreads) {
             const long long l = t0 + i;
             double c[3], sv[3];
@@ -247,9 +252,17 @@ __global__ void __launch_bounds__(kFusedThreads)
     }
 }
 
+// source records per shared-memory tile for `total` source cells: all of them
+// when they fit (a smaller footprint lets more CTAs share an SM), else DtTile::N
 template <class Real>
-inline size_t dt_fused_smem() {
-    return sizeof(FusedRec<Real>) * (size_t)DtTile<Real>::N + sizeof(double) * kFusedThreads * 7;
+inline int dt_fused_tile(long long total) {
+    const long long t = (total + 31) / 32 * 32;
+    return (int)(t < DtTile<Real>::N ? t : DtTile<Real>::N);
+}
+
+template <class Real>
+inline size_t dt_fused_smem(long long total) {
+    return sizeof(FusedRec<Real>) * (size_t)dt_fused_tile<Real>(total) + sizeof(double) * kFusedThreads * 7;
 }
 
 }  // namespace lddmm

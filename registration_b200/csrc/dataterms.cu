@@ -175,10 +175,23 @@ int dt_value_fused(const DataArgs& a, Workspace& ws, cudaStream_t st) {
     FusedCoef cf{};
     for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
     for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
-    return launch_fused(dt_value_fused_kernel<Real, KIND, PDEG, D>, fs, a.nbatch, dt_fused_smem<Real>(),
-                        dt_fused_smem<Real>(), st, a.ncorner, a.norm, a.v, (long long)a.nv, a.cells,
+    const long long total = a.nc + a.nc2;
+    return launch_fused(dt_value_fused_kernel<Real, KIND, PDEG, D>, fs, a.nbatch, dt_fused_smem<Real>(total),
+                        dt_fused_smem<Real>(DtTile<Real>::N), st, a.ncorner, a.norm, a.v, (long long)a.nv, a.cells,
                         (long long)a.nc, a.c2, a.s2, (long long)a.nc2, a.eps1, a.eps2, ks.scale, cf, fs, epart,
-                        a.energy, a.vstride);
+                        a.energy, a.vstride, dt_fused_tile<Real>(total));
+}
+
+int dt_value_resident_clusters(long long nc, long long nc2, int d, int fp64) {
+    const FusedShape fs = fused_shape(nc);
+    auto go = [&](auto D) {
+        constexpr int D_ = decltype(D)::value;
+        return fp64 ? fused_resident_clusters(dt_value_fused_kernel<double, KGAUSS, 0, D_>, fs,
+                                              dt_fused_smem<double>(nc + nc2), dt_fused_smem<double>(DtTile<double>::N))
+                    : fused_resident_clusters(dt_value_fused_kernel<float, KGAUSS, 0, D_>, fs,
+                                              dt_fused_smem<float>(nc + nc2), dt_fused_smem<float>(DtTile<float>::N));
+    };
+    return d == 2 ? go(IC<2>{}) : go(IC<3>{});
 }
 
 template <class Real>

@@ -58,7 +58,10 @@ constexpr long long kFusedMaxPoints = LDDMM_FUSED_MAX_POINTS;
 constexpr int kFusedMaxCluster = 8;
 // targets per CTA before the cluster grows: every CTA of a full cluster then
 // owns <= 64 targets, each target spread over >= 8 source groups
-constexpr int kFusedTargetsPerCta = 32;
+#ifndef LDDMM_FUSED_TPC
+#define LDDMM_FUSED_TPC 32
+#endif
+constexpr int kFusedTargetsPerCta = LDDMM_FUSED_TPC;
 
 struct FusedShape {
     int C;    // CTAs in the cluster
@@ -497,37 +500,62 @@ inline size_t fused_dyn_smem(long long n, int D) {
 // Launches `kernel` on `nbatch` clusters of fs.C CTAs (cluster b works on
 // problem b of a batch) with `smem` bytes of dynamic shared memory
 // (`max_smem`: the kernel's opt-in limit, at least smem).
-template <class Kern, class... Args>
-int launch_fused(Kern kernel, const FusedShape& fs, int nbatch, size_t smem, size_t max_smem, cudaStream_t st,
-                 Args... args) {
-    // the shared-memory opt-in, once per (device, kernel)
+// The shared-memory opt-in of a fused kernel, once per (device, kernel).
+template <class Kern>
+int fused_prepare(Kern kernel, size_t max_smem) {
     static std::mutex mu;
     static std::set<std::pair<int, const void*>> done;
     int dev = 0;
     LDDMM_TRY(cuda_check(cudaGetDevice(&dev), "fused: cudaGetDevice"));
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
-        if (done.count(key) == 0) {
-            LDDMM_TRY(cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      (int)max_smem),
-                                 "fused kernel attribute"));
-            done.insert(key);
-        }
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
+    if (done.count(key) == 0) {
+        LDDMM_TRY(cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem),
+                             "fused kernel attribute"));
+        done.insert(key);
     }
+    return LDDMM_OK;
+}
+
+// cluster launch configuration: nbatch clusters of fs.C CTAs; attr must outlive cfg
+inline cudaLaunchConfig_t fused_config(const FusedShape& fs, int nbatch, size_t smem, cudaStream_t st,
+                                       cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(fs.C * nbatch, 1, 1);
     cfg.blockDim = dim3(kFusedThreads, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = fs.C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    return cfg;
+}
+
+template <class Kern, class... Args>
+int launch_fused(Kern kernel, const FusedShape& fs, int nbatch, size_t smem, size_t max_smem, cudaStream_t st,
+                 Args... args) {
+    LDDMM_TRY(fused_prepare(kernel, max_smem));
+    cudaLaunchAttribute attr[1];
+    const cudaLaunchConfig_t cfg = fused_config(fs, nbatch, smem, st, attr);
     return cuda_check(cudaLaunchKernelEx(&cfg, kernel, args...), "fused launch");
+}
+
+// How many clusters of `kernel` (fs.C CTAs, smem bytes each) are resident on the device at once
+// (0 on error).
+template <class Kern>
+int fused_resident_clusters(Kern kernel, const FusedShape& fs, size_t smem, size_t max_smem) {
+    if (fused_prepare(kernel, max_smem) != LDDMM_OK) return 0;
+    cudaLaunchAttribute attr[1];
+    const cudaLaunchConfig_t cfg = fused_config(fs, 1, smem, 0, attr);
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)kernel, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return clusters;
 }
 
 }  // namespace lddmm

@@ -816,10 +816,20 @@ int lddmm_shoot_along_batch_f64(const double* x0, int64_t n, int d, const double
     return shoot_entry<double>(a, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
-int lddmm_trial_batch_size(int64_t n, int d, int64_t nc, int64_t nc2) {
+int lddmm_trial_batch_size(int64_t n, int d, int64_t nc, int64_t nc2, int shot_fp64, int value_fp64) {
     if (n < 1 || d < 2 || d > 3 || n > kFusedMaxPoints || !dt_fused_fits(nc, nc2)) return 1;
-    const int clusters = device_info().sms / fused_shape(n).C;
-    return std::max(1, std::min(kTrialBatch, clusters));
+    // clusters of the batched shot and value kernels resident at once (the Gaussian
+    // instances stand for the kernel family)
+    auto shot = [&](auto D) {
+        constexpr int D_ = decltype(D)::value;
+        const FusedShape fs = fused_shape(n);
+        return shot_fp64 ? fused_resident_clusters(shoot_fused_kernel<double, KGAUSS, 0, D_>, fs,
+                                                   fused_dyn_smem<double>(n, D_), fused_dyn_smem<double>(kFusedMaxPoints, 3))
+                         : fused_resident_clusters(shoot_fused_kernel<float, KGAUSS, 0, D_>, fs,
+                                                   fused_dyn_smem<float>(n, D_), fused_dyn_smem<float>(kFusedMaxPoints, 3));
+    };
+    const int c = std::min(d == 2 ? shot(IC<2>{}) : shot(IC<3>{}), dt_value_resident_clusters(nc, nc2, d, value_fp64));
+    return std::max(1, std::min(kTrialBatch, c));
 }
 
 size_t lddmm_covector_f32c_workspace(int64_t n, int d, int T) { return cov_ws<float>(n, d, T); }

@@ -112,11 +112,12 @@ def shoot_along_batch(x0, at, dir_, eps, KparDiff, regweight=1.0, at_try=None, x
     return outs["at_try"], outs["xt"], outs["energy"]
 
 
-def trial_batch_size(n, d, ncells, ncells_target):
+def trial_batch_size(n, d, ncells, ncells_target, shot_precision="fp32c", value_precision="fp64"):
     """Step sizes that one batched trial launch evaluates side by side (1: the
     problem is too large for the single-cluster kernels, batches would run one
     step size after the other)."""
-    return max(1, _lib.query("lddmm_trial_batch_size", int(n), int(d), int(ncells), int(ncells_target)))
+    return max(1, _lib.query("lddmm_trial_batch_size", int(n), int(d), int(ncells), int(ncells_target),
+                             int(shot_precision == "fp64"), int(value_precision == "fp64")))
 
 
 def metric_dots(xt, g1, g2s, KparDiff):

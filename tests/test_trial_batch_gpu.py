@@ -88,8 +88,12 @@ def test_trial_batch_size_and_arguments():
     from registration_b200 import kernelFunctions as kf
     from registration_b200 import pointEvolution as ev
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    assert ev.trial_batch_size(256, 2, 256, 256) == min(16, sms // 8)
-    assert ev.trial_batch_size(40, 3, 80, 80) == min(16, sms // 2)
+    # bounded by the resident clusters of both kernels (8 CTAs each at 256 points, 2 at 40) and by 24
+    for shot, value in (("fp32c", "fp64"), ("fp64", "fp64"), ("fp32c", "fp32c")):
+        b256 = ev.trial_batch_size(256, 2, 256, 256, shot, value)
+        b40 = ev.trial_batch_size(40, 3, 80, 80, shot, value)
+        assert 8 <= b256 <= min(24, 2 * sms // 8), (shot, value, b256)
+        assert b256 <= b40 <= 24, (shot, value, b40)
     assert ev.trial_batch_size(700, 3, 1000, 1000) == 1
     assert ev.trial_batch_size(256, 2, 256, 4000) == 1       # the value would leave the single-cluster kernel
     x0, at, dr = _problem(20, 2, 3, 1)
