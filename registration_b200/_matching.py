@@ -261,11 +261,15 @@ class DeviceMatching:
         problem is small, so a batch costs about what one trial step does)."""
         g = self._graph
         out = g["out_buf"]   # [deformation energies, raw data terms] (2, B): written in place
+        # the step sizes come from, and the values go to, pinned host buffers: the
+        # two copies are part of the replay
+        g["eps"].copy_(g["eps_host"], non_blocking=True)
         _, xt, _ = evol.shoot_along_batch(self.x0, g["at"], g["dir"], g["eps"], self.param.KparDiff,
                                           regweight=self.regweight, at_try=g["atTry"], xt=g["xt"],
                                           energy=out[0])
         _dt.value_batch(self.param.errorType, xt[:, -1], self._dshape, self._tc, self._tv, self._Kval,
                         energy_out=out[1])
+        g["out_host"].copy_(out, non_blocking=True)
         return out
 
     def expectTrials(self, dir, steps):
@@ -338,9 +342,10 @@ class DeviceMatching:
                                "atTry": torch.empty((B, T, n, d), dtype=torch.float64, device=dev),
                                "xt": torch.empty((B, T + 1, n, d), dtype=torch.float64, device=dev),
                                "out_buf": torch.empty((2, B), dtype=torch.float64, device=dev),
-                               "eps_host": torch.empty(B, dtype=torch.float64).pin_memory(),
+                               "eps_host": torch.full((B,), float(eps), dtype=torch.float64).pin_memory(),
                                "out_host": torch.empty((2, B), dtype=torch.float64).pin_memory(),
                                "at_src": self.at, "dir_src": dir.diff, "cache": {}}
+            g["eps_np"], g["out_np"] = g["eps_host"].numpy(), g["out_host"].numpy()
             # capture on a side stream with the low-level calls (the torch.cuda.graph
             # context manager also collects garbage and empties the allocator cache)
             side = torch.cuda.Stream()
@@ -370,16 +375,15 @@ class DeviceMatching:
         if eps not in cache:
             self._materialize_try()     # the slots are about to be overwritten
             ladder = self._trial_ladder(eps, cache, dir.diff)
-            g["eps_host"].numpy()[:] = ladder
-            g["eps"].copy_(g["eps_host"], non_blocking=True)
+            g["eps_np"][:] = ladder
             g["graph"].replay()
             self.calls["trial_batches"] = self.calls.get("trial_batches", 0) + 1
-            g["out_host"].copy_(g["out_buf"], non_blocking=True)
             torch.cuda.current_stream().synchronize()
-            host = g["out_host"].numpy()
+            ereg, raw = g["out_np"].tolist()
             cache.clear()
             for b, e in enumerate(ladder):
-                cache.setdefault(e, (b, float(host[0, b]), float(host[1, b])))
+                if e not in cache:
+                    cache[e] = (b, ereg[b], raw[b])
         b, ereg, raw = cache[eps]
         objTry = self._combine(ereg, raw)
         if self._auto:
