@@ -415,7 +415,7 @@ def curve_measure(iters, sig_err, steps, warmup, with_cpu):
         tc = time.perf_counter() - t0
         cpu = {"value": 1.0 / tc, "unit": "matches/s", "cores": os.cpu_count(), "kind": "port",
                "sample": "one whole match (FP64 numpy + C/OpenMP loops)", "final_energy": rcm.obj}
-    # a match is about 1,300 short launches and 300 host read-backs driven from
+    # a match is about 1,100 short launches and 160 host read-backs driven from
     # Python: host-bound and sensitive to load on the (shared) host, so the
     # median step is the value
     med = float(np.median(times))
