@@ -108,33 +108,14 @@ LDDMM_D void dt_fused_cell(long long l, int ncorner, const double* v, long long 
     }
 }
 
-// Every CTA computes the cell geometry it needs itself (a few cached loads per
-// cell), so the only cluster barrier is the one of the final energy sum.
-template <class Real, int KIND, int PDEG, int D>
-__global__ void __launch_bounds__(kFusedThreads)
-    dt_value_fused_kernel(int ncorner, int norm, const double* __restrict__ v, long long nv,
-                          const int64_t* __restrict__ cells, long long nc, const double* __restrict__ c2,
-                          const double* __restrict__ s2, long long nc2, double eps1, double eps2, double scale,
-                          FusedCoef cf, FusedShape fs, double* epart, double* energy, long long vstride,
-                          int tile) {
-    extern __shared__ __align__(32) unsigned char fused_smem[];
-    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
-    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * tile);
-    double* scratch = red + kFusedThreads;
-    const int rank = (int)cluster_rank();
+// Packing frame of a data term: the centre of the bounding box of all cell
+// centres of S1 (from the vertices) and S2 (exact min / max, the same in every
+// CTA); block-wide, `scratch` holds 6 * kFusedThreads doubles.
+template <int D>
+LDDMM_D void dt_fused_frame(int ncorner, const double* v, long long nv, const int64_t* cells, long long nc,
+                            const double* c2, const double* s2, long long nc2, double* scratch, double* ctr) {
     const int tid = threadIdx.x;
-    const int local = tid % fs.tpt, g = tid / fs.tpt;
-    const long long k = (long long)rank * fs.nc + local;
-    const bool owner = local < fs.nc && k < nc;
-    // batched values: cluster b evaluates the vertex set v + b vstride into energy[b]
-    const long long b = blockIdx.x / fs.C;
-    v += b * vstride;
-    energy += b;
-    epart += b * kFusedMaxCluster;
-    Real pk[5];
-    for (int j = 0; j < 5; ++j) pk[j] = (Real)cf.pk[j];
     const long long total = nc + nc2;
-    // packing frame: centre of the bounding box of all cell centres (exact min / max)
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     bool any = false;
     for (long long l = tid; l < total; l += kFusedThreads) {
@@ -161,10 +142,39 @@ __global__ void __launch_bounds__(kFusedThreads)
             }
         __syncthreads();
     }
-    double ctr[3];
     for (int j = 0; j < 3; ++j)
         ctr[j] = j < D ? 0.5 * (scratch[(2 * j) * kFusedThreads] + scratch[(2 * j + 1) * kFusedThreads]) : 0.0;
     __syncthreads();
+}
+
+// Every CTA computes the cell geometry it needs itself (a few cached loads per
+// cell), so the only cluster barrier is the one of the final energy sum.
+template <class Real, int KIND, int PDEG, int D>
+__global__ void __launch_bounds__(kFusedThreads)
+    dt_value_fused_kernel(int ncorner, int norm, const double* __restrict__ v, long long nv,
+                          const int64_t* __restrict__ cells, long long nc, const double* __restrict__ c2,
+                          const double* __restrict__ s2, long long nc2, double eps1, double eps2, double scale,
+                          FusedCoef cf, FusedShape fs, double* epart, double* energy, long long vstride,
+                          int tile) {
+    extern __shared__ __align__(32) unsigned char fused_smem[];
+    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
+    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * tile);
+    double* scratch = red + kFusedThreads;
+    const int rank = (int)cluster_rank();
+    const int tid = threadIdx.x;
+    const int local = tid % fs.tpt, g = tid / fs.tpt;
+    const long long k = (long long)rank * fs.nc + local;
+    const bool owner = local < fs.nc && k < nc;
+    // batched values: cluster b evaluates the vertex set v + b vstride into energy[b]
+    const long long b = blockIdx.x / fs.C;
+    v += b * vstride;
+    energy += b;
+    epart += b * kFusedMaxCluster;
+    Real pk[5];
+    for (int j = 0; j < 5; ++j) pk[j] = (Real)cf.pk[j];
+    const long long total = nc + nc2;
+    double ctr[3];
+    dt_fused_frame<D>(ncorner, v, nv, cells, nc, c2, s2, nc2, scratch, ctr);
     // the target cell of this thread
     Real xk[3] = {0, 0, 0}, uk[3] = {0, 0, 0};
     double wk = 0.0;
@@ -250,6 +260,140 @@ __global__ void __launch_bounds__(kFusedThreads)
         for (int r = 0; r < fs.C; ++r) sum += __ldcg(epart + r);
         energy[0] = sum;
     }
+}
+
+// Single-launch data-term GRADIENT (NormGradient, surfaces.py:1069-1087,
+// 1150-1182, 1228-1276; curves.py:594-650) for small shapes: the pair sums of
+// the general path's gradient sweep (targets: the S1 cells, sources: S1 with
+// sign +1 and S2 with sign -1) for each CTA's own cells, the per-cell z1 / dz1
+// (dt_grad_row) into global memory, one cluster barrier, then the vertex
+// gather of each CTA's share of the vertices (dt_gather_vertex).
+constexpr int kDtGradOut = 7;   // accumulators: 2 d + 1 at most
+
+template <class Real, int KIND, int PDEG, int QDEG, int D>
+__global__ void __launch_bounds__(kFusedThreads)
+    dt_grad_fused_kernel(int ncorner, int norm, const double* __restrict__ v, long long nv,
+                         const int64_t* __restrict__ cells, long long nc, const double* __restrict__ c2,
+                         const double* __restrict__ s2, long long nc2, double eps1, double eps2, double scale,
+                         double dzscale, FusedCoef cf, FusedShape fs, int tile, const int64_t* __restrict__ vptr,
+                         const int64_t* __restrict__ vidx, double* z1, double* dz1, double* __restrict__ px) {
+    extern __shared__ __align__(32) unsigned char fused_smem[];
+    FusedRec<Real>* rec = reinterpret_cast<FusedRec<Real>*>(fused_smem);
+    double* red = reinterpret_cast<double*>(fused_smem + sizeof(FusedRec<Real>) * tile);
+    double* scratch = red + kFusedThreads * kDtGradOut;
+    const int rank = (int)cluster_rank();
+    const int tid = threadIdx.x;
+    const int local = tid % fs.tpt, g = tid / fs.tpt;
+    const long long k = (long long)rank * fs.nc + local;
+    const bool owner = local < fs.nc && k < nc;
+    Real pk[5], pq[4];
+    for (int j = 0; j < 5; ++j) pk[j] = (Real)cf.pk[j];
+    for (int j = 0; j < 4; ++j) pq[j] = (Real)cf.pq[j];
+    const long long total = nc + nc2;
+    double ctr[3];
+    dt_fused_frame<D>(ncorner, v, nv, cells, nc, c2, s2, nc2, scratch, ctr);
+    // the target cell of this thread: position, and s (current) or n = s / a (varifold)
+    Real xk[3] = {0, 0, 0}, uk[3] = {0, 0, 0};
+    double sk[3] = {0, 0, 0};
+    if (owner) {
+        double ck[3], q = 0.0;
+        dt_fused_cell<D>(k, ncorner, v, nv, cells, nc, c2, s2, ck, sk);
+        for (int j = 0; j < D; ++j) {
+            xk[j] = (Real)((ck[j] - ctr[j]) * scale);
+            q += sk[j] * sk[j];
+        }
+        const double ak = sqrt(q + eps1);
+        for (int j = 0; j < 3; ++j) uk[j] = (Real)(norm == NCURRENT ? sk[j] : sk[j] / ak);
+    }
+    FusedAcc<Real, kDtGradOut> acc;
+    acc.zero();
+    constexpr int FOLD = sizeof(Real) == 4 ? 32 : 1 << 30;
+    for (long long t0 = 0; t0 < total; t0 += tile) {
+        const int len = (int)(total - t0 < tile ? total - t0 : tile);
+        for (int i = tid; i < len; i += kFusedThreads) {
+            const long long l = t0 + i;
+            double c[3], sv[3];
+            dt_fused_cell<D>(l, ncorner, v, nv, cells, nc, c2, s2, c, sv);
+            dt_fused_record<Real>(rec[i], c, sv, D, l < nc ? eps1 : eps2, l < nc ? 1.0 : -1.0, norm, scale, ctr);
+        }
+        __syncthreads();
+        if (owner) {
+            const int jb0 = (int)((long long)g * len / fs.S), je0 = (int)((long long)(g + 1) * len / fs.S);
+            for (int jb = jb0; jb < je0; jb += FOLD) {
+                acc.begin_fold();
+                const int je = jb + FOLD < je0 ? jb + FOLD : je0;
+                for (int j = jb; j < je; ++j) {
+                    Real y[3], w[6], dx[3];
+                    fused_pos<Real>(rec[j], y);
+                    fused_vals<Real>(rec[j], w);
+                    Real r2 = 0;
+#pragma unroll
+                    for (int q = 0; q < D; ++q) {
+                        dx[q] = xk[q] - y[q];
+                        r2 = q == 0 ? dx[q] * dx[q] : r2 + dx[q] * dx[q];
+                    }
+                    Real kv, fv;
+                    kboth<Real, KIND, PDEG, QDEG>(pk, pq, r2, kv, fv);
+                    if (norm == NVARIFOLD) {
+                        const Real dn = uk[0] * w[0] + uk[1] * w[1] + uk[2] * w[2];
+                        const Real wk = kv * w[3];
+                        const Real ca = 2 * dn * wk;
+#pragma unroll
+                        for (int q = 0; q < D; ++q) acc.fma(q, ca, w[q]);
+                        acc.fma(D, wk, (Real)1 - dn * dn);
+                        const Real wf = fv * w[3] * ((Real)1 + dn * dn);
+#pragma unroll
+                        for (int q = 0; q < D; ++q) acc.fma(D + 1 + q, wf, dx[q]);
+                    } else if (norm == NCURRENT) {
+                        Real dot = 0;
+#pragma unroll
+                        for (int q = 0; q < D; ++q) {
+                            acc.fma(q, kv, w[q]);
+                            dot = q == 0 ? uk[0] * w[0] : dot + uk[q] * w[q];
+                        }
+                        const Real gq = fv * dot;
+#pragma unroll
+                        for (int q = 0; q < D; ++q) acc.fma(D + q, gq, dx[q]);
+                    } else {
+                        acc.fma(0, kv, w[0]);
+                        const Real gq = fv * w[0];
+#pragma unroll
+                        for (int q = 0; q < D; ++q) acc.fma(1 + q, gq, dx[q]);
+                    }
+                }
+                acc.end_fold();
+            }
+        }
+        __syncthreads();
+    }
+    // z1 / dz1 of the target cell: source groups in order, in FP64
+    if (owner)
+#pragma unroll
+        for (int c = 0; c < kDtGradOut; ++c) red[(g * fs.tpt + local) * kDtGradOut + c] = acc.value(c);
+    __syncthreads();
+    if (owner && g == 0) {
+        double a[kDtGradOut];
+        for (int c = 0; c < kDtGradOut; ++c) {
+            a[c] = 0.0;
+            for (int gg = 0; gg < fs.S; ++gg) a[c] += red[(gg * fs.tpt + local) * kDtGradOut + c];
+        }
+        double z[3], dz[3];
+        dt_grad_row(norm, a, sk, D, eps1, dzscale, z, dz);
+        for (int j = 0; j < D; ++j) {
+            __stcg(z1 + k * D + j, z[j]);
+            __stcg(dz1 + k * D + j, dz[j]);
+        }
+    }
+    cluster_sync_acq_rel();
+    // the vertex gather: vertices [rank nv / C, (rank + 1) nv / C)
+    const long long q0 = (long long)rank * nv / fs.C, q1 = (long long)(rank + 1) * nv / fs.C;
+    for (long long q = q0 + tid; q < q1; q += kFusedThreads)
+        dt_gather_vertex<true>(q, ncorner, v, nv, D, cells, nc, vptr, vidx, z1, dz1, px);
+}
+
+template <class Real>
+inline size_t dt_grad_fused_smem(int tile) {
+    return sizeof(FusedRec<Real>) * (size_t)tile + sizeof(double) * kFusedThreads * (kDtGradOut + 6);
 }
 
 // source records per shared-memory tile for `total` source cells: all of them

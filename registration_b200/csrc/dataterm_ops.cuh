@@ -527,40 +527,51 @@ static __global__ void dt_grad_combine_kernel(int norm, const double* __restrict
     }
 }
 
-// px[v] = 2 sum over (cell, corner) entries of v of the corner contribution.
+// px[q] = 2 sum over the (cell, corner) entries of vertex q of the corner contribution.
+// L2ONLY: z1 / dz1 were written by other CTAs of the same launch (loads bypass L1).
+template <bool L2ONLY = false>
+LDDMM_D void dt_gather_vertex(long long q, int ncorner, const double* __restrict__ v, long long nv, int d,
+                              const int64_t* __restrict__ cells, long long nc, const int64_t* __restrict__ vptr,
+                              const int64_t* __restrict__ vidx, const double* z1, const double* dz1,
+                              double* __restrict__ px) {
+    double acc[3] = {0, 0, 0};
+    const long long b = vptr[q], e = vptr[q + 1];
+    for (long long k = b; k < e; ++k) {
+        const long long code = vidx[k];
+        if (code < 0 || code >= nc * ncorner) continue;
+        const long long f = code / ncorner;
+        const int corner = (int)(code - f * ncorner);
+        double z[3] = {0, 0, 0}, dz[3] = {0, 0, 0};
+        for (int j = 0; j < d; ++j) {
+            z[j] = L2ONLY ? __ldcg(z1 + f * d + j) : z1[f * d + j];
+            dz[j] = L2ONLY ? __ldcg(dz1 + f * d + j) : dz1[f * d + j];
+        }
+        if (ncorner == 3) {
+            // opposite edge of the corner: x2-x1, x0-x2, x1-x0
+            const int ia = (corner + 2) % 3, ib = (corner + 1) % 3;
+            const long long va = cells[f * 3 + ia], vb = cells[f * 3 + ib];
+            if (va < 0 || va >= nv || vb < 0 || vb >= nv) continue;
+            double ed[3];
+            for (int j = 0; j < 3; ++j) ed[j] = v[va * 3 + j] - v[vb * 3 + j];
+            const double cr[3] = {ed[1] * z[2] - ed[2] * z[1], ed[2] * z[0] - ed[0] * z[2],
+                                  ed[0] * z[1] - ed[1] * z[0]};
+            for (int j = 0; j < 3; ++j) acc[j] += dz[j] - cr[j];
+        } else {
+            const double sgn = corner == 0 ? -1.0 : 1.0;
+            for (int j = 0; j < d; ++j) acc[j] += dz[j] + sgn * z[j];
+        }
+    }
+    for (int j = 0; j < d; ++j) px[q * d + j] = 2 * acc[j];
+}
+
 static __global__ void dt_gather_kernel(int ncorner, const double* __restrict__ v, long long nv, int d,
                                         const int64_t* __restrict__ cells, long long nc,
                                         const int64_t* __restrict__ vptr, const int64_t* __restrict__ vidx,
                                         const double* __restrict__ z1, const double* __restrict__ dz1,
                                         double* __restrict__ px) {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv;
-         q += (long long)gridDim.x * blockDim.x) {
-        double acc[3] = {0, 0, 0};
-        const long long b = vptr[q], e = vptr[q + 1];
-        for (long long k = b; k < e; ++k) {
-            const long long code = vidx[k];
-            if (code < 0 || code >= nc * ncorner) continue;
-            const long long f = code / ncorner;
-            const int corner = (int)(code - f * ncorner);
-            const double* z = z1 + f * d;
-            const double* dz = dz1 + f * d;
-            if (ncorner == 3) {
-                // opposite edge of the corner: x2-x1, x0-x2, x1-x0
-                const int ia = (corner + 2) % 3, ib = (corner + 1) % 3;
-                const long long va = cells[f * 3 + ia], vb = cells[f * 3 + ib];
-                if (va < 0 || va >= nv || vb < 0 || vb >= nv) continue;
-                double ed[3];
-                for (int j = 0; j < 3; ++j) ed[j] = v[va * 3 + j] - v[vb * 3 + j];
-                const double cr[3] = {ed[1] * z[2] - ed[2] * z[1], ed[2] * z[0] - ed[0] * z[2],
-                                      ed[0] * z[1] - ed[1] * z[0]};
-                for (int j = 0; j < 3; ++j) acc[j] += dz[j] - cr[j];
-            } else {
-                const double sgn = corner == 0 ? -1.0 : 1.0;
-                for (int j = 0; j < d; ++j) acc[j] += dz[j] + sgn * z[j];
-            }
-        }
-        for (int j = 0; j < d; ++j) px[q * d + j] = 2 * acc[j];
-    }
+         q += (long long)gridDim.x * blockDim.x)
+        dt_gather_vertex(q, ncorner, v, nv, d, cells, nc, vptr, vidx, z1, dz1, px);
 }
 
 

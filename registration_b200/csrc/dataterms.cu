@@ -182,6 +182,26 @@ int dt_value_fused(const DataArgs& a, Workspace& ws, cudaStream_t st) {
                         a.energy, a.vstride, dt_fused_tile<Real>(total));
 }
 
+// Gradient (and value, if asked) of small shapes: one cluster launch each (dataterm_fused.cuh).
+template <class Real, int KIND, int PDEG, int QDEG, int D>
+int dt_grad_fused(const DataArgs& a, Workspace& ws, cudaStream_t st) {
+    if (a.energy != nullptr) LDDMM_TRY((dt_value_fused<Real, KIND, PDEG, D>(a, ws, st)));
+    const FusedShape fs = fused_shape(a.nc);
+    double* z1 = ws.take<double>((size_t)a.nc * a.d);
+    double* dz1 = ws.take<double>((size_t)a.nc * a.d);
+    if (ws.measuring()) return LDDMM_OK;
+    const KScale ks = kernel_scale<Real>(KIND, a.order, a.sigma);
+    FusedCoef cf{};
+    for (int j = 0; j < 5; ++j) cf.pk[j] = ks.pk[j];
+    for (int j = 0; j < 4; ++j) cf.pq[j] = ks.pq[j];
+    const double fac = a.ncorner == 3 ? 1.0 / 3.0 : 0.5;
+    const int tile = dt_fused_tile<Real>(a.nc + a.nc2);
+    return launch_fused(dt_grad_fused_kernel<Real, KIND, PDEG, QDEG, D>, fs, 1, dt_grad_fused_smem<Real>(tile),
+                        dt_grad_fused_smem<Real>(DtTile<Real>::N), st, a.ncorner, a.norm, a.v, (long long)a.nv,
+                        a.cells, (long long)a.nc, a.c2, a.s2, (long long)a.nc2, a.eps1, a.eps2, ks.scale,
+                        fac * ks.dscale, cf, fs, tile, a.vptr, a.vidx, z1, dz1, a.px);
+}
+
 int dt_value_resident_clusters(long long nc, long long nc2, int d, int fp64) {
     const FusedShape fs = fused_shape(nc);
     auto go = [&](auto D) {
@@ -218,6 +238,8 @@ int dt_run(const DataArgs& a, Workspace& ws, cudaStream_t st) {
             constexpr int K_ = decltype(kind)::value, P_ = decltype(pdeg)::value, Q_ = decltype(qdeg)::value,
                           D_ = decltype(D)::value;
             if (fused && a.d == D_) return dt_value_fused<Real, K_, P_, D_>(a, ws, st);
+            if (a.px != nullptr && a.nbatch == 1 && dt_fused_fits(a.nc, a.nc2) && a.d == D_)
+                return dt_grad_fused<Real, K_, P_, Q_, D_>(a, ws, st);
             if (a.nc <= kSmallTargets) return dt_impl<Real, K_, P_, Q_, D_, true>(a, ws, st);
             return dt_impl<Real, K_, P_, Q_, D_>(a, ws, st);
         });
