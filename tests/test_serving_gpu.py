@@ -412,7 +412,10 @@ def _curve_requests(idx, iters=8):
 def test_served_curves_alone_equal_mix_and_match_curve_matching():
     """Curve requests (edges, d = 2) follow CurveMatching's protocol (cg's
     first step 10): alone == in the mix bit for bit, and the same decisions as
-    the single-problem CurveMatching with FP64 line-search values."""
+    the single-problem CurveMatching with FP64 line-search values.  The single
+    problem's FP32c kernel sums run in other kernels (single-launch ones for
+    these sizes) than the served ragged launches, so the final energies agree
+    to the FP32c scale of the objective, 1e-5 of obj0."""
     from registration_b200 import curves as cv
     from registration_b200 import serving
     from registration_b200.curveMatching import CurveMatching
@@ -427,4 +430,4 @@ def test_served_curves_alone_equal_mix_and_match_curve_matching():
                            maxIter=8, saveRate=0, lineSearchPrecision="fp64")
         cm.optimizeMatching()
         assert b["iters"] == cm.iter
-        assert abs(b["obj"] - cm.obj) <= 1e-5 * abs(cm.obj), (b["obj"], cm.obj)
+        assert abs(b["obj"] - cm.obj) <= 1e-5 * abs(cm.obj0), (b["obj"], cm.obj, cm.obj0)
