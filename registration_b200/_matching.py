@@ -380,10 +380,8 @@ class DeviceMatching:
             self.calls["trial_batches"] = self.calls.get("trial_batches", 0) + 1
             torch.cuda.current_stream().synchronize()
             ereg, raw = g["out_np"].tolist()
-            cache.clear()
-            for b, e in enumerate(ladder):
-                if e not in cache:
-                    cache[e] = (b, ereg[b], raw[b])
+            # the ladder's step sizes are distinct
+            cache = g["cache"] = dict(zip(ladder, zip(range(len(ladder)), ereg, raw)))
         b, ereg, raw = cache[eps]
         objTry = self._combine(ereg, raw)
         if self._auto:

@@ -130,3 +130,18 @@ def test_best_trial_copied_out_of_its_slot_only_when_needed():
     assert m.obj == 5.0 and torch.equal(m.at, g["atTry"][2]) and torch.equal(m.xt, g["xt"][2])
     g["atTry"][2].fill_(-1.0)                            # the slot is reused by the next batch
     assert torch.equal(m.at, torch.arange(16.0, 24.0).reshape(2, 4))
+
+
+def test_ladders_are_distinct_and_full():
+    """A batch's step sizes are distinct (they key the batch's values) and fill it."""
+    rng = np.random.default_rng(0)
+    d = object()
+    for B in (1, 2, 3, 5, 8, 13, 16, 20, 24, 32):
+        m = _bare(B)
+        for _ in range(200):
+            e, p = float(10 ** rng.uniform(-8, 3)), float(10 ** rng.uniform(-9, -5))
+            m._hint = (d, [e, p])
+            lad = m._trial_ladder(e, {}, d)
+            assert len(lad) == B and len(set(lad)) == B
+            grow = m._trial_ladder(1.25 * lad[min(3, B - 1)], set(lad), d)
+            assert len(grow) == B and len(set(grow)) == B
