@@ -85,4 +85,4 @@ void laplacian_tables(int order, double P[5], double Q[4], double Rr[3], bool ex
 }  // namespace lddmm
 
 extern "C" const char* lddmm_last_error(void) { return lddmm::g_last_error.c_str(); }
-extern "C" int lddmm_abi_version(void) { return 2; }
+extern "C" int lddmm_abi_version(void) { return 3; }
