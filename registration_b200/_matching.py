@@ -23,6 +23,13 @@ step is kept instead of re-shooting it in endOfIteration, and getGradient
 runs the adjoint on that stored trajectory instead of re-shooting inside
 landmarkHamiltonianGradient (the shots are deterministic, so they would be
 bit-identical).
+
+With cudaGraphs (the default) the trial steps are replayed from a CUDA graph;
+for problems small enough to run on one thread-block cluster a replay
+evaluates a batch of the step sizes the line search asks for next (one
+cluster each, side by side), and the gradient is replayed from a second
+graph.  Every value, and so every decision and the accepted trace, equals
+the eager path's.
 """
 import contextlib
 import gc
