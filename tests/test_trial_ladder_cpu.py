@@ -145,3 +145,35 @@ def test_ladders_are_distinct_and_full():
             assert len(lad) == B and len(set(lad)) == B
             grow = m._trial_ladder(1.25 * lad[min(3, B - 1)], set(lad), d)
             assert len(grow) == B and len(set(grow)) == B
+
+
+def test_cg_hints_the_probe_it_then_tries():
+    """cg's optional hint names, before each line search, the first step size
+    and the tiny-step probe; when the first trial fails, the probe cg tries is
+    exactly the hinted value (so a batch holding it answers the call)."""
+
+    class Hinted(_Recorder):
+        def __init__(self):
+            super().__init__(1)
+            self.hints, self.first = [], []
+
+        def expectTrials(self, dir, steps):
+            self.hints.append((dir, list(steps)))
+
+        def updateTry(self, dir, eps, objRef=None):
+            if self.hints and self.hints[-1][0] is dir:
+                self.first.append((len(self.hints), float(eps)))
+            return super().updateTry(dir, eps, objRef)
+
+    r = Hinted()
+    r.x = np.array([30.0, -20.0, 15.0])      # far from the optimum: the first steps overshoot
+    CG.cg(r, verb=False, maxIter=15, epsInit=10.0)
+    assert r.hints
+    probes = 0
+    for i, (d, steps) in enumerate(r.hints, start=1):
+        tried = [e for k, e in r.first if k == i]
+        assert tried and tried[0] == steps[0]          # the first trial is the hinted step
+        if len(tried) > 1 and tried[1] < steps[0] / 1000:
+            assert tried[1] == steps[1]                # the probe is the hinted value
+            probes += 1
+    assert probes >= 1
