@@ -22,7 +22,10 @@ int sweep_slots() {
 // Problems with at most this many targets use the SMALL tile shape of the
 // packed operators that have one (more, smaller items: the large shape would
 // leave most SMs idle).
-constexpr long long kSmallTargets = 4096;
+#ifndef LDDMM_SMALL_TARGETS
+#define LDDMM_SMALL_TARGETS 4096
+#endif
+constexpr long long kSmallTargets = LDDMM_SMALL_TARGETS;
 
 struct SinglePlan {
     long long n_tpad, m_pad;
