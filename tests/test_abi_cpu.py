@@ -61,3 +61,30 @@ def test_invalid_arguments_are_rejected_before_any_launch(lib):
     assert L.lddmm_applyk_f32c(null, 10, null, 10, null, 3, 3, 0.0, 10, null, null, 0, null) == -1
     assert L.lddmm_applykdifft_f32c(null, 10, null, 10, null, null, 1, 3, 3, 1.0, 0, null, null, 0, null) == -1
     assert b"not differentiable" in L.lddmm_last_error()
+
+
+def test_new_entry_points_reject_bad_arguments_on_the_host(lib):
+    """The trial-step, batch and metric-dot entry points check their arguments
+    before anything is enqueued (here, with no GPU, a host-side answer)."""
+    from registration_b200 import _lib
+    L = _lib.load()
+    null = ctypes.c_void_p(0)
+    # batch sizes outside [1, 4096]: no workspace, argument error
+    assert L.lddmm_shoot_along_batch_f32c_workspace(100, 2, 10, 0) == 0
+    assert L.lddmm_shoot_along_batch_f32c_workspace(100, 2, 10, 5000) == 0
+    assert L.lddmm_shoot_along_batch_f32c_workspace(100, 2, 10, 16) > 0
+    assert L.lddmm_shoot_along_batch_f32c(null, 100, 2, null, null, null, 0, 10, 0.0, 1.0, 10, 1.0, null, null, null,
+                                          null, 0, null) == -1
+    assert L.lddmm_dataterm_value_batch_f64_workspace(2, 0, 100, 2, 100, 100, 10, 0) == 0
+    # a batch of values needs a vertex stride of at least nv * d
+    assert L.lddmm_dataterm_value_batch_f64(2, 0, null, 100, 2, null, 100, null, null, 100, 1.0, 10, 1e-10, 1e-10, 3,
+                                            10, null, null, 0, null) == -1
+    assert b"vertex_stride" in L.lddmm_last_error()
+    # metric dots: 1 to 8 directions
+    ptrs = (ctypes.c_void_p * 9)()
+    assert L.lddmm_metric_dots_f32c_workspace(100, 2, 10, 9) == 0
+    assert L.lddmm_metric_dots_f32c(null, 100, 2, 10, null, ptrs, 9, 1.0, 10, null, null, 0, null) == -1
+    assert L.lddmm_metric_dots_f32c_workspace(100, 2, 10, 2) > 0
+    # too large for the single-cluster kernels: one step size per launch
+    assert L.lddmm_trial_batch_size(100000, 3, 200000, 200000, 0, 1) == 1
+    assert L.lddmm_trial_batch_size(256, 4, 256, 256, 0, 1) == 1
