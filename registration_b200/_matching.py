@@ -420,29 +420,48 @@ class DeviceMatching:
         _, dat = evol.covector(xt, at, px1, self.param.KparDiff, self.regweight, with_dat=True)
         return dat / (coeff * self.Tsize)
 
+    def _gradient_graph_body(self, g, coeff):
+        """The gradient, and the two metric products cg asks for next,
+        <g, g> and <g, g_prev> (dotProduct's kernel on the same inputs), into
+        pinned host memory; g_prev is the previous gradient of this graph."""
+        dat = self._gradient_body(g["xt"], g["at"], coeff)
+        if g["dots"]:
+            d = evol.metric_dots(g["xt"], dat, [dat, g["prev"]], self.param.KparDiff)
+            g["dots_host"].copy_(d, non_blocking=True)
+            g["prev"].copy_(dat)
+        return dat
+
     def _graph_gradient(self, coeff):
         """The data-term gradient, the adjoint and the scaling replayed from a CUDA
         graph (the same kernels on copies of xt and at: bit-identical to the
-        eager path); a small problem's dozen launches become one."""
+        eager path); a small problem's dozen launches become one.  With the FP32c
+        metric products the replay also forms <g, g> and <g, g_prev>, which
+        dotProduct then returns for cg's dot(grd, [grd, grdOld])."""
         g = self._grad_graph
         if g is None or g["coeff"] != coeff:
             import types
+            K = self.param.KparDiff
             g = self._grad_graph = {"coeff": coeff, "xt": self.xt.clone(), "at": self.at.clone(),
-                                    "xt_src": self.xt, "at_src": self.at, "owner": types.SimpleNamespace()}
+                                    "xt_src": self.xt, "at_src": self.at, "owner": types.SimpleNamespace(),
+                                    "dots": K.precision == 'fp32c' and self.npt <= 2048,
+                                    "prev": torch.zeros_like(self.at),
+                                    "dots_host": torch.zeros(2, dtype=torch.float64).pin_memory(),
+                                    "last": None, "last_prev": None}
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             graph = torch.cuda.CUDAGraph()
             with _gc_paused(), torch.cuda.stream(side):
                 with workspace.scope(g["owner"]):
-                    self._gradient_body(g["xt"], g["at"], coeff)
+                    self._gradient_graph_body(g, coeff)
                 with workspace.scope(g["owner"]):
                     graph.capture_begin()
                     try:
-                        g["dat"] = self._gradient_body(g["xt"], g["at"], coeff)
+                        g["dat"] = self._gradient_graph_body(g, coeff)
                     finally:
                         graph.capture_end()
             torch.cuda.current_stream().wait_stream(side)
             g["graph"] = graph
+            g["prev_valid"] = False   # the warm-up call left a gradient in "prev"
         if g["xt_src"] is not self.xt:
             g["xt"].copy_(self.xt)
             g["xt_src"] = self.xt
@@ -450,7 +469,35 @@ class DeviceMatching:
             g["at"].copy_(self.at)
             g["at_src"] = self.at
         g["graph"].replay()
-        return g["dat"].clone()
+        out = g["dat"].clone()
+        # the products of this replay: <out, out> and, if the previous gradient
+        # of this graph is known, <out, previous>
+        g["last_prev"] = g["last"] if g["prev_valid"] else None
+        g["last"], g["prev_valid"] = out, True
+        g["dots_xt"] = self.xt
+        return out
+
+    def _precomputed_dots(self, g1, g2):
+        """dotProduct's values from the last gradient replay, when the call is
+        dot(g, [g or g_prev, ...]) on that gradient g (g_prev: the previous
+        gradient or a copyDir of it) and the trajectory has not changed."""
+        g = self._grad_graph
+        if g is None or not g["dots"] or g["last"] is None or g1.diff is not g["last"]:
+            return None
+        if g.get("dots_xt") is not self.xt:
+            return None
+        idx = []
+        for gr in g2:
+            src = gr.diff if gr.diff is g["last"] else getattr(gr, "copied_from", None)
+            if gr.diff is g["last"]:
+                idx.append(0)
+            elif g["last_prev"] is not None and (gr.diff is g["last_prev"] or src is g["last_prev"]):
+                idx.append(1)
+            else:
+                return None
+        torch.cuda.current_stream().synchronize()
+        vals = g["dots_host"].numpy()
+        return np.array([vals[i] for i in idx])
 
     def addProd(self, dir1, dir2, beta):
         d = Direction()
@@ -462,6 +509,7 @@ class DeviceMatching:
         d = Direction()
         d.diff = dir0.diff.clone()
         d.aff = np.copy(dir0.aff)
+        d.copied_from = dir0.diff   # lets dotProduct recognise cg's grdOld
         return d
 
     def randomDir(self):
@@ -474,6 +522,9 @@ class DeviceMatching:
         """sum_t <g2_t, K(x_t) g1_t> (surfaceMatching.py:353-377), FP64 on the device."""
         self.calls["dotProduct"] += 1
         K = self.param.KparDiff
+        pre = self._precomputed_dots(g1, g2)
+        if pre is not None:
+            return pre
         if K.precision == 'fp32c' and self.npt <= 2048 and 1 <= len(g2) <= 8:
             # all T steps and directions in two launches (pointEvolution.metric_dots)
             return evol.metric_dots(self.xt, g1.diff, [gr.diff for gr in g2], K).cpu().numpy()
